@@ -1,0 +1,697 @@
+// clifft_gpu.cu -- C ABI of the sm_100a Schrodinger-VM backend (include/clifft_gpu.h).
+//
+// Host side: program validation and upload, launch-shape selection, scratch
+// and output management around the persistent interpreter kernel of
+// svm_kernel.cuh.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "clifft_gpu.h"
+#include "svm_kernel.cuh"
+
+using namespace cgpu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CUDA_OK(expr)                                                                         \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            throw ApiError(_e == cudaErrorMemoryAllocation ? CLIFFT_GPU_ENOMEM : CLIFFT_GPU_ECUDA, \
+                           std::string(#expr) + ": " + cudaGetErrorString(_e));               \
+    } while (0)
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return CLIFFT_GPU_OK;
+    } catch (const ApiError& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CLIFFT_GPU_EINVAL;
+    }
+}
+
+[[noreturn]] void invalid(const std::string& m) { throw ApiError(CLIFFT_GPU_EINVAL, m); }
+
+constexpr uint32_t kMaxPeakRank = 34;  // 2^34 complex FP32 = 128 GiB: beyond one B200's HBM per shot
+constexpr uint32_t kMaxWords = 4;      // frame width: num_qubits <= 256
+
+uint16_t rd16(const uint8_t* p) {
+    uint16_t v;
+    std::memcpy(&v, p, 2);
+    return v;
+}
+uint32_t rd32(const uint8_t* p) {
+    uint32_t v;
+    std::memcpy(&v, p, 4);
+    return v;
+}
+uint64_t rd64(const uint8_t* p) {
+    uint64_t v;
+    std::memcpy(&v, p, 8);
+    return v;
+}
+
+// Checks the invariants the reference executor asserts
+// (src/clifft/svm/svm_kernels.inl: axis < active_k for array ops, EXPAND on
+// axis k, active measurements on axis k-1, pool indices in range) so that no
+// launch can index outside the program or the statevector.
+uint32_t validate(const clifft_program_image& im) {
+    if (im.num_words != (im.num_qubits + 63) / 64 && !(im.num_qubits == 0 && im.num_words <= 1))
+        invalid("num_words must equal ceil(num_qubits / 64)");
+    if (im.num_words > kMaxWords) invalid("num_qubits > 256 is not supported by the CUDA backend");
+    if (im.peak_rank > kMaxPeakRank) invalid("peak_rank too large for one GPU");
+    if (im.total_meas_slots < im.num_measurements) invalid("total_meas_slots < num_measurements");
+    if (im.num_instructions && !im.instructions) invalid("null instruction array");
+    const uint32_t nq = std::max<uint32_t>(im.num_qubits, 1);
+    const uint32_t frame_bits = std::max<uint32_t>(im.num_words, 1) * 64;
+    for (uint32_t s = 0; s < im.num_noise_sites; ++s)
+        if (im.noise_site_offsets[s] > im.noise_site_offsets[s + 1] ||
+            im.noise_site_offsets[s + 1] > im.num_noise_channels)
+            invalid("noise site offsets out of range");
+    for (uint32_t d = 0; d < im.num_detector_lists; ++d)
+        for (uint32_t i = im.detector_offsets[d]; i < im.detector_offsets[d + 1]; ++i)
+            if (im.detector_targets[i] >= im.total_meas_slots) invalid("detector target out of range");
+    for (uint32_t d = 0; d < im.num_observable_lists; ++d)
+        for (uint32_t i = im.observable_offsets[d]; i < im.observable_offsets[d + 1]; ++i)
+            if (im.observable_targets[i] >= im.total_meas_slots) invalid("observable target out of range");
+    for (uint32_t r = 0; r < im.num_readout_noise; ++r)
+        if (im.readout_meas_idx[r] >= im.total_meas_slots) invalid("readout entry out of range");
+    for (uint32_t n = 0; n < im.num_u2 * 4; ++n)
+        if (im.u2_out[n] > 3) invalid("U2 out state out of range");
+    for (uint32_t n = 0; n < im.num_u4 * 16; ++n)
+        if (im.u4_out[n] > 15) invalid("U4 out state out of range");
+
+    uint32_t k = 0, peak = 0;
+    for (uint32_t pc = 0; pc < im.num_instructions; ++pc) {
+        const uint8_t* I = im.instructions + size_t(pc) * 32;
+        uint32_t op = I[0];
+        const uint32_t fl = I[2];
+        const uint32_t a1 = rd16(I + 4), a2 = rd16(I + 6);
+        const uint32_t p0 = rd32(I + 8), p1 = rd32(I + 12);
+        auto bad = [&](const char* what) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "instruction %u (opcode %u): %s (active_k=%u)", pc, I[0], what, k);
+            invalid(buf);
+        };
+        if (op >= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED)
+            op -= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED - CLIFFT_OP_MEAS_DORMANT_STATIC;
+        switch (op) {
+            case CLIFFT_OP_FRAME_CNOT:
+            case CLIFFT_OP_FRAME_CZ:
+            case CLIFFT_OP_FRAME_SWAP:
+                if (a1 >= frame_bits || a2 >= frame_bits) bad("axis beyond the frame");
+                break;
+            case CLIFFT_OP_FRAME_H:
+            case CLIFFT_OP_FRAME_S:
+            case CLIFFT_OP_FRAME_S_DAG:
+                if (a1 >= frame_bits) bad("axis beyond the frame");
+                break;
+            case CLIFFT_OP_ARRAY_CNOT:
+            case CLIFFT_OP_ARRAY_CZ:
+            case CLIFFT_OP_ARRAY_SWAP:
+                if (a1 >= k || a2 >= k || a1 == a2) bad("two-axis array op needs distinct active axes");
+                break;
+            case CLIFFT_OP_ARRAY_MULTI_CNOT:
+            case CLIFFT_OP_ARRAY_MULTI_CZ: {
+                uint64_t m = rd64(I + 8);
+                if (a1 >= k) bad("multi-gate pivot axis not active");
+                if (k < 64 && (m >> k)) bad("multi-gate mask has dormant axes");
+                if ((m >> a1) & 1u) bad("multi-gate mask contains its own pivot");
+                break;
+            }
+            case CLIFFT_OP_ARRAY_H:
+            case CLIFFT_OP_ARRAY_S:
+            case CLIFFT_OP_ARRAY_S_DAG:
+                if (a1 >= k) bad("array op on a dormant axis");
+                break;
+            case CLIFFT_OP_ARRAY_T:
+            case CLIFFT_OP_ARRAY_T_DAG:
+            case CLIFFT_OP_ARRAY_ROT:
+                if (a1 >= frame_bits) bad("axis beyond the frame");
+                break;
+            case CLIFFT_OP_ARRAY_U2:
+                if (a1 >= frame_bits) bad("axis beyond the frame");
+                if (p0 >= im.num_u2) bad("U2 constant-pool index out of range");
+                break;
+            case CLIFFT_OP_ARRAY_U4:
+                if (!(a1 < a2 && a2 < k)) bad("U4 needs axis_lo < axis_hi < active_k");
+                if (p0 >= im.num_u4) bad("U4 constant-pool index out of range");
+                break;
+            case CLIFFT_OP_EXPAND:
+            case CLIFFT_OP_EXPAND_T:
+            case CLIFFT_OP_EXPAND_T_DAG:
+            case CLIFFT_OP_EXPAND_ROT:
+                if (a1 != k) bad("EXPAND must target axis active_k");
+                if (a1 >= frame_bits) bad("axis beyond the frame");
+                ++k;
+                peak = std::max(peak, k);
+                if (k > im.peak_rank) bad("EXPAND exceeds peak_rank");
+                break;
+            case CLIFFT_OP_MEAS_DORMANT_STATIC:
+            case CLIFFT_OP_MEAS_DORMANT_RANDOM:
+                if (p0 >= im.total_meas_slots) bad("classical index out of range");
+                if (!(fl & CLIFFT_FLAG_IDENTITY) && a1 >= frame_bits) bad("axis beyond the frame");
+                break;
+            case CLIFFT_OP_MEAS_ACTIVE_DIAGONAL:
+            case CLIFFT_OP_MEAS_ACTIVE_INTERFERE:
+                if (k == 0 || a1 != k - 1) bad("active measurement must target axis active_k-1");
+                if (p0 >= im.total_meas_slots) bad("classical index out of range");
+                --k;
+                break;
+            case CLIFFT_OP_SWAP_MEAS_INTERFERE:
+                if (k == 0 || a2 != k - 1 || a1 > a2) bad("swap-measure must target axis active_k-1");
+                if (p0 >= im.total_meas_slots) bad("classical index out of range");
+                --k;
+                break;
+            case CLIFFT_OP_APPLY_PAULI:
+                if (p0 >= im.num_pauli_masks) bad("Pauli mask index out of range");
+                if (p1 >= im.total_meas_slots) bad("condition index out of range");
+                break;
+            case CLIFFT_OP_NOISE:
+                if (p0 >= im.num_noise_sites) bad("noise site out of range");
+                break;
+            case CLIFFT_OP_NOISE_BLOCK:
+                if (uint64_t(p0) + p1 > im.num_noise_sites) bad("noise block out of range");
+                break;
+            case CLIFFT_OP_READOUT_NOISE:
+                if (p0 >= im.num_readout_noise) bad("readout entry out of range");
+                break;
+            case CLIFFT_OP_DETECTOR:
+            case CLIFFT_OP_POSTSELECT:
+                if (p0 >= im.num_detector_lists) bad("detector list out of range");
+                if (p1 >= im.num_detectors) bad("detector index out of range");
+                break;
+            case CLIFFT_OP_OBSERVABLE:
+                if (p0 >= im.num_observable_lists) bad("observable list out of range");
+                if (p1 >= im.num_observables) bad("observable index out of range");
+                break;
+            case CLIFFT_OP_EXP_VAL:
+                if (p0 >= im.num_exp_val_masks) bad("EXP_VAL mask out of range");
+                if (p1 >= im.num_exp_vals) bad("EXP_VAL index out of range");
+                break;
+            default:
+                bad("unknown opcode");
+        }
+    }
+    (void)nq;
+    return peak;
+}
+
+
+// Device-side scratch freed in stream order when the call ends.
+struct StreamBuffers {
+    cudaStream_t stream;
+    std::vector<void*> ptrs;
+    explicit StreamBuffers(cudaStream_t s) : stream(s) {}
+    void* alloc(size_t bytes) {
+        void* p = nullptr;
+        if (bytes == 0) return nullptr;
+        CUDA_OK(cudaMallocAsync(&p, bytes, stream));
+        ptrs.push_back(p);
+        return p;
+    }
+    ~StreamBuffers() {
+        for (void* p : ptrs) cudaFreeAsync(p, stream);
+    }
+};
+
+}  // namespace
+
+struct clifft_gpu_program {
+    clifft_program_image meta{};  // counts only (host pointers dropped)
+    DevProg dev{};
+    void* blob = nullptr;
+    size_t blob_bytes = 0;
+    std::vector<uint8_t> expected_host;
+    int device = 0;
+};
+
+namespace {
+
+struct BlobBuilder {
+    std::vector<uint8_t> bytes;
+    template <typename T>
+    size_t put(const T* src, size_t count) {
+        size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + count * sizeof(T));
+        if (count) std::memcpy(bytes.data() + off, src, count * sizeof(T));
+        return off;
+    }
+};
+
+template <typename T>
+const T* at(void* base, size_t off) {
+    return reinterpret_cast<const T*>(static_cast<uint8_t*>(base) + off);
+}
+
+// kernel table ----------------------------------------------------------
+using KernelFn = void (*)(const DevProg, const KParams);
+
+template <typename R>
+KernelFn pick_kernel(bool warp, uint32_t nw) {
+    if (warp) {
+        if (nw <= 1) return svm_sample_kernel<R, WarpGroup, 1>;
+        if (nw <= 2) return svm_sample_kernel<R, WarpGroup, 2>;
+        return svm_sample_kernel<R, WarpGroup, 4>;
+    }
+    if (nw <= 1) return svm_sample_kernel<R, CtaGroup, 1>;
+    if (nw <= 2) return svm_sample_kernel<R, CtaGroup, 2>;
+    return svm_sample_kernel<R, CtaGroup, 4>;
+}
+
+struct LaunchPlan {
+    KernelFn fn;
+    bool warp;
+    int threads;      // block size
+    int groups_per_block;
+    int blocks;
+    size_t smem;
+    bool state_in_smem;
+    uint64_t state_stride;
+    uint32_t nw_words;
+};
+
+uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : (nw <= 2 ? 2 : 4); }
+
+LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
+                       uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words) {
+    LaunchPlan L{};
+    const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
+    const uint64_t stride = uint64_t(1) << p.meta.peak_rank;
+    const size_t state_bytes = stride * amp;
+    const size_t rec_bytes = size_t(rec_words + det_words + obs_words) * 4;
+    int dev = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    int smem_optin = 0, sms = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t smem_cap = size_t(smem_optin) - 1024;
+
+    bool warp;
+    if (group_req == 32)
+        warp = true;
+    else if (group_req > 32)
+        warp = false;
+    else
+        warp = state_bytes <= 8192;  // k <= 10 (FP32) / k <= 9 (FP64): one warp per shot
+    L.warp = warp;
+    L.nw_words = nw_template(p.meta.num_words);
+    L.fn = precision == CLIFFT_GPU_FP32 ? pick_kernel<float>(warp, L.nw_words)
+                                        : pick_kernel<double>(warp, L.nw_words);
+    cudaFuncAttributes fa{};
+    CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
+    const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
+
+    if (warp) {
+        L.threads = std::min(256, max_threads);
+        L.groups_per_block = L.threads / 32;
+        size_t group = (state_bytes + rec_bytes + 15) & ~size_t(15);
+        // fall back to fewer warps per block if the slabs do not fit
+        while (L.groups_per_block > 1 &&
+               group * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64 > smem_cap) {
+            L.groups_per_block /= 2;
+            L.threads = L.groups_per_block * 32;
+        }
+        L.state_in_smem = group * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64 <= smem_cap;
+    } else {
+        int t = group_req > 32 ? int(group_req) : (state_bytes <= (size_t(32) << 10) ? 256 : 512);
+        if (!(group_req > 32) && state_bytes > (size_t(160) << 10)) t = 1024;
+        L.threads = std::min(t, max_threads);
+        L.groups_per_block = 1;
+        size_t group = (state_bytes + rec_bytes + 15) & ~size_t(15);
+        L.state_in_smem = group + 3 * 8 * (L.threads / 32) + 64 <= smem_cap;
+    }
+    const size_t group_bytes =
+        ((L.state_in_smem ? state_bytes : 0) + rec_bytes + 15) & ~size_t(15);
+    L.smem = group_bytes * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64;
+    if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
+    CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(L.smem)));
+    int per_sm = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)L.fn, L.threads, L.smem));
+    if (per_sm < 1) invalid("kernel does not fit on an SM with this launch shape");
+    const uint64_t groups_needed = (shots + L.groups_per_block - 1) / L.groups_per_block;
+    uint64_t blocks = uint64_t(per_sm) * sms;
+    if (!L.state_in_smem) {
+        // global slabs: bound the resident state to ~half of free HBM
+        size_t free_b = 0, total_b = 0;
+        CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
+        uint64_t max_groups = std::max<uint64_t>(1, (free_b / 2) / std::max<size_t>(state_bytes, 1));
+        blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, max_groups / L.groups_per_block));
+    }
+    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, groups_needed));
+    L.blocks = int(blocks);
+    L.state_stride = stride;
+    return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* clifft_gpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* clifft_gpu_backend_name(void) {
+    static thread_local std::string name;
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        name = "unavailable:no CUDA device";
+        return name.c_str();
+    }
+    if (prop.major != 10) {
+        name = std::string("unavailable:sm_") + std::to_string(prop.major) + std::to_string(prop.minor) +
+               " (this build targets sm_100a)";
+        return name.c_str();
+    }
+    name = std::string("cuda:sm_100a:") + prop.name;
+    return name.c_str();
+}
+
+int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out) {
+    return guarded([&] {
+        if (!image || !out) invalid("null argument");
+        *out = nullptr;
+        const clifft_program_image& im = *image;
+        uint32_t peak = validate(im);
+        (void)peak;
+        auto p = std::make_unique<clifft_gpu_program>();
+        p->meta = im;
+        const uint32_t nw = std::max<uint32_t>(im.num_words, 1);
+        const uint32_t nwt = nw_template(nw);
+        // masks are widened to the kernel's template width (zero words above num_words)
+        auto widen = [&](const uint64_t* src, uint32_t count) {
+            std::vector<uint64_t> w(size_t(count) * nwt, 0);
+            for (uint32_t i = 0; i < count; ++i)
+                for (uint32_t j = 0; j < im.num_words; ++j) w[size_t(i) * nwt + j] = src[size_t(i) * im.num_words + j];
+            return w;
+        };
+        std::vector<double> psum(im.num_noise_sites);
+        for (uint32_t s = 0; s < im.num_noise_sites; ++s) {
+            double acc = 0.0;  // same summation order as exec_noise (svm_kernels.inl:1898-1901)
+            for (uint32_t c = im.noise_site_offsets[s]; c < im.noise_site_offsets[s + 1]; ++c)
+                acc += im.noise_channel_prob[c];
+            psum[s] = acc;
+        }
+        BlobBuilder b;
+        size_t o_instr = b.put(im.instructions, size_t(im.num_instructions) * 32);
+        auto px = widen(im.pauli_x, im.num_pauli_masks), pz = widen(im.pauli_z, im.num_pauli_masks);
+        auto ex = widen(im.exp_val_x, im.num_exp_val_masks), ez = widen(im.exp_val_z, im.num_exp_val_masks);
+        auto cx = widen(im.noise_channel_x, im.num_noise_channels);
+        auto cz = widen(im.noise_channel_z, im.num_noise_channels);
+        size_t o_px = b.put(px.data(), px.size()), o_pz = b.put(pz.data(), pz.size());
+        size_t o_ps = b.put(im.pauli_sign, im.num_pauli_masks);
+        size_t o_ex = b.put(ex.data(), ex.size()), o_ez = b.put(ez.data(), ez.size());
+        size_t o_es = b.put(im.exp_val_sign, im.num_exp_val_masks);
+        std::vector<uint32_t> site_off(im.noise_site_offsets, im.noise_site_offsets + im.num_noise_sites + 1);
+        if (im.num_noise_sites == 0) site_off.assign(1, 0);
+        size_t o_so = b.put(site_off.data(), site_off.size());
+        size_t o_psum = b.put(psum.data(), psum.size());
+        size_t o_cp = b.put(im.noise_channel_prob, im.num_noise_channels);
+        size_t o_cx = b.put(cx.data(), cx.size()), o_cz = b.put(cz.data(), cz.size());
+        size_t o_hz = b.put(im.noise_hazards, im.num_noise_sites);
+        size_t o_rm = b.put(im.readout_meas_idx, im.num_readout_noise);
+        size_t o_rp = b.put(im.readout_prob, im.num_readout_noise);
+        std::vector<uint32_t> det_off(im.detector_offsets, im.detector_offsets + im.num_detector_lists + 1);
+        std::vector<uint32_t> obs_off(im.observable_offsets, im.observable_offsets + im.num_observable_lists + 1);
+        if (im.num_detector_lists == 0) det_off.assign(1, 0);
+        if (im.num_observable_lists == 0) obs_off.assign(1, 0);
+        size_t o_do = b.put(det_off.data(), det_off.size());
+        size_t o_dt = b.put(im.detector_targets, det_off.back());
+        size_t o_oo = b.put(obs_off.data(), obs_off.size());
+        size_t o_ot = b.put(im.observable_targets, obs_off.back());
+        size_t o_u2 = b.put(im.u2_data, size_t(im.num_u2) * CLIFFT_U2_DOUBLES_PER_NODE);
+        size_t o_u2o = b.put(im.u2_out, size_t(im.num_u2) * 4);
+        size_t o_u4 = b.put(im.u4_data, size_t(im.num_u4) * CLIFFT_U4_DOUBLES_PER_NODE);
+        size_t o_u4o = b.put(im.u4_out, size_t(im.num_u4) * 16);
+        p->expected_host.assign(im.expected_observables, im.expected_observables + im.num_expected_observables);
+        size_t o_exo = b.put(p->expected_host.data(), p->expected_host.size());
+        b.bytes.resize(b.bytes.size() + 256);
+        CUDA_OK(cudaGetDevice(&p->device));
+        CUDA_OK(cudaMalloc(&p->blob, b.bytes.size()));
+        p->blob_bytes = b.bytes.size();
+        CUDA_OK(cudaMemcpy(p->blob, b.bytes.data(), b.bytes.size(), cudaMemcpyHostToDevice));
+        DevProg& d = p->dev;
+        void* B = p->blob;
+        d.instr = at<uint4>(B, o_instr);
+        d.n_instr = im.num_instructions;
+        d.nw = nwt;
+        d.peak = im.peak_rank;
+        d.num_meas = im.num_measurements;
+        d.slots = im.total_meas_slots;
+        d.num_det = im.num_detectors;
+        d.num_obs = im.num_observables;
+        d.num_exp = im.num_exp_vals;
+        d.pauli_x = at<uint64_t>(B, o_px);
+        d.pauli_z = at<uint64_t>(B, o_pz);
+        d.pauli_sign = at<uint8_t>(B, o_ps);
+        d.exp_x = at<uint64_t>(B, o_ex);
+        d.exp_z = at<uint64_t>(B, o_ez);
+        d.exp_sign = at<uint8_t>(B, o_es);
+        d.n_sites = im.num_noise_sites;
+        d.site_off = at<uint32_t>(B, o_so);
+        d.site_psum = at<double>(B, o_psum);
+        d.chan_prob = at<double>(B, o_cp);
+        d.chan_x = at<uint64_t>(B, o_cx);
+        d.chan_z = at<uint64_t>(B, o_cz);
+        d.hazards = at<double>(B, o_hz);
+        d.ro_meas = at<uint32_t>(B, o_rm);
+        d.ro_prob = at<double>(B, o_rp);
+        d.det_off = at<uint32_t>(B, o_do);
+        d.det_tg = at<uint32_t>(B, o_dt);
+        d.obs_off = at<uint32_t>(B, o_oo);
+        d.obs_tg = at<uint32_t>(B, o_ot);
+        d.u2 = at<double>(B, o_u2);
+        d.u2_out = at<uint8_t>(B, o_u2o);
+        d.u4 = at<double>(B, o_u4);
+        d.u4_out = at<uint8_t>(B, o_u4o);
+        d.n_expected = im.num_expected_observables;
+        d.expected = at<uint8_t>(B, o_exo);
+        // drop host pointers from the retained metadata
+        clifft_program_image& m = p->meta;
+        m.instructions = nullptr;
+        m.pauli_x = m.pauli_z = m.exp_val_x = m.exp_val_z = m.noise_channel_x = m.noise_channel_z = nullptr;
+        m.pauli_sign = m.exp_val_sign = m.u2_out = m.u4_out = m.expected_observables = nullptr;
+        m.noise_site_offsets = m.readout_meas_idx = m.detector_offsets = m.detector_targets = nullptr;
+        m.observable_offsets = m.observable_targets = nullptr;
+        m.noise_channel_prob = m.noise_hazards = m.readout_prob = m.u2_data = m.u4_data = nullptr;
+        *out = p.release();
+    });
+}
+
+void clifft_gpu_free(clifft_gpu_program* prog) {
+    if (!prog) return;
+    if (prog->blob) {
+        cudaDeviceSynchronize();
+        cudaFree(prog->blob);
+    }
+    delete prog;
+}
+
+uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog) { return prog ? prog->meta.peak_rank : 0; }
+uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog) { return prog ? prog->blob_bytes : 0; }
+
+int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, clifft_gpu_outputs* out) {
+    return guarded([&] {
+        if (!prog || !args || !out) invalid("null argument");
+        const clifft_program_image& m = prog->meta;
+        const uint64_t shots = args->shots;
+        if (args->precision != CLIFFT_GPU_FP32 && args->precision != CLIFFT_GPU_FP64)
+            invalid("precision must be CLIFFT_GPU_FP32 or CLIFFT_GPU_FP64");
+        if (args->group_threads != 0 && (args->group_threads % 32 != 0 || args->group_threads > 1024))
+            invalid("group_threads must be 0 or a multiple of 32 up to 1024");
+        const bool dev_ptrs = (args->flags & CLIFFT_GPU_DEVICE_PTRS) != 0;
+        const bool forced_meas = (args->flags & CLIFFT_GPU_FORCED_MEAS) != 0;
+        const bool forced_faults = (args->flags & CLIFFT_GPU_FORCED_FAULTS) != 0;
+        if (forced_meas && !args->forced_meas) invalid("CLIFFT_GPU_FORCED_MEAS needs forced_meas");
+        if (forced_faults && (!args->fault_offsets || !args->readout_offsets))
+            invalid("CLIFFT_GPU_FORCED_FAULTS needs fault_offsets and readout_offsets");
+        out->passed_shots = 0;
+        out->logical_errors = 0;
+        out->dust_clamps = 0;
+        out->kernel_launches = 0;
+        out->kernel_ms = 0.f;
+        if (shots == 0) return;
+        CUDA_OK(cudaSetDevice(prog->device));
+        cudaStream_t st = static_cast<cudaStream_t>(args->stream);
+        StreamBuffers buf(st);
+
+        // host-side validation of forced-fault inputs (bounds only)
+        std::vector<uint32_t> h_foff, h_roff;
+        if (forced_faults && !dev_ptrs) {
+            for (uint64_t s = 0; s < shots; ++s) {
+                if (args->fault_offsets[s] > args->fault_offsets[s + 1] ||
+                    args->readout_offsets[s] > args->readout_offsets[s + 1])
+                    invalid("forced-fault offsets must be non-decreasing");
+                for (uint32_t f = args->fault_offsets[s]; f < args->fault_offsets[s + 1]; ++f) {
+                    if (args->fault_sites[f] >= m.num_noise_sites) invalid("forced fault site out of range");
+                    if (f > args->fault_offsets[s] && args->fault_sites[f] <= args->fault_sites[f - 1])
+                        invalid("forced fault sites must be strictly ascending per shot");
+                }
+            }
+        }
+
+        const uint32_t rec_words = (m.total_meas_slots + 31) / 32;
+        const uint32_t det_words = (m.num_detectors + 31) / 32;
+        const uint32_t obs_words = (m.num_observables + 31) / 32;
+        LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words,
+                                   det_words, obs_words);
+
+        KParams K{};
+        K.shots = shots;
+        K.first_shot = args->first_shot;
+        K.seed = args->seed;
+        K.dust_eps = args->dust_eps > 0.0 ? args->dust_eps : (args->precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
+        K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
+                  (forced_meas ? KF_FORCED_MEAS : 0) | (forced_faults ? KF_FORCED_FAULTS : 0) |
+                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0);
+        K.rec_words = rec_words;
+        K.det_words = det_words;
+        K.obs_words = obs_words;
+        K.meas_out_words = (m.num_measurements + 63) / 64;
+        K.det_out_words = (m.num_detectors + 63) / 64;
+        K.obs_out_words = (m.num_observables + 63) / 64;
+        K.state_in_smem = L.state_in_smem ? 1 : 0;
+        K.state_stride = L.state_stride;
+        const size_t amp = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
+        if (!L.state_in_smem)
+            K.state_global = buf.alloc(size_t(L.blocks) * L.groups_per_block * L.state_stride * amp);
+        const size_t n_counters = 3 + m.num_observables;
+        auto* scratch = static_cast<unsigned long long*>(buf.alloc((2 + n_counters) * 8 + 64));
+        CUDA_OK(cudaMemsetAsync(scratch, 0, (2 + n_counters) * 8 + 64, st));
+        K.work_counter = scratch;
+        K.error_word = reinterpret_cast<int*>(scratch + 1);
+        K.counters = scratch + 2;
+
+        // inputs
+        auto stage_in = [&](const void* src, size_t bytes) -> const void* {
+            if (!src || bytes == 0) return nullptr;
+            if (dev_ptrs) return src;
+            void* d = buf.alloc(bytes);
+            CUDA_OK(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st));
+            return d;
+        };
+        if (forced_meas)
+            K.forced_meas = static_cast<const uint8_t*>(stage_in(args->forced_meas, shots * m.total_meas_slots));
+        if (forced_faults) {
+            uint64_t nf = dev_ptrs ? 0 : args->fault_offsets[shots];
+            uint64_t nr = dev_ptrs ? 0 : args->readout_offsets[shots];
+            K.fault_off = static_cast<const uint32_t*>(stage_in(args->fault_offsets, (shots + 1) * 4));
+            K.ro_off = static_cast<const uint32_t*>(stage_in(args->readout_offsets, (shots + 1) * 4));
+            if (dev_ptrs) {
+                K.fault_sites = args->fault_sites;
+                K.fault_chan = args->fault_channels;
+                K.ro_entries = args->readout_entries;
+            } else {
+                K.fault_sites = static_cast<const uint32_t*>(stage_in(args->fault_sites, nf * 4));
+                K.fault_chan = static_cast<const uint32_t*>(stage_in(args->fault_channels, nf * 4));
+                K.ro_entries = static_cast<const uint32_t*>(stage_in(args->readout_entries, nr * 4));
+            }
+        }
+
+        // outputs
+        struct Out {
+            void* host;
+            void* dev;
+            size_t bytes;
+        };
+        std::vector<Out> outs;
+        auto stage_out = [&](void* host, size_t bytes) -> void* {
+            if (!host || bytes == 0) return nullptr;
+            if (dev_ptrs) return host;
+            void* d = buf.alloc(bytes);
+            outs.push_back({host, d, bytes});
+            return d;
+        };
+        K.out_meas = static_cast<uint64_t*>(stage_out(out->meas, shots * K.meas_out_words * 8));
+        K.out_det = static_cast<uint64_t*>(stage_out(out->det, shots * K.det_out_words * 8));
+        K.out_obs = static_cast<uint64_t*>(stage_out(out->obs, shots * K.obs_out_words * 8));
+        K.out_exp = static_cast<double*>(stage_out(out->exp_vals, shots * m.num_exp_vals * 8));
+        K.out_survived = static_cast<uint8_t*>(stage_out(out->survived, shots));
+        if (args->flags & CLIFFT_GPU_TRACE) {
+            K.out_meas_prob = static_cast<double*>(stage_out(out->meas_prob, shots * m.total_meas_slots * 8));
+            K.out_log_prob = static_cast<double*>(stage_out(out->log_prob, shots * 8));
+            K.out_final_k = static_cast<uint32_t*>(stage_out(out->final_k, shots * 4));
+            K.out_final_gamma = static_cast<double*>(stage_out(out->final_gamma, shots * 16));
+            // px/pz are written at the kernel's template width; narrow below
+            const uint32_t nwt = L.nw_words;
+            K.out_final_px = static_cast<uint64_t*>(buf.alloc(out->final_px ? shots * nwt * 8 : 0));
+            K.out_final_pz = static_cast<uint64_t*>(buf.alloc(out->final_pz ? shots * nwt * 8 : 0));
+            K.dump_shots = std::min<uint64_t>(out->dump_shots, shots);
+            K.out_final_v = static_cast<double*>(
+                stage_out(out->final_v, K.dump_shots * (uint64_t(1) << m.peak_rank) * 16));
+        }
+
+        cudaEvent_t e0, e1;
+        CUDA_OK(cudaEventCreate(&e0));
+        CUDA_OK(cudaEventCreate(&e1));
+        CUDA_OK(cudaEventRecord(e0, st));
+        L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
+        CUDA_OK(cudaGetLastError());
+        CUDA_OK(cudaEventRecord(e1, st));
+
+        for (auto& o : outs) CUDA_OK(cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, st));
+        std::vector<unsigned long long> hs(2 + n_counters);
+        CUDA_OK(cudaMemcpyAsync(hs.data(), scratch, hs.size() * 8, cudaMemcpyDeviceToHost, st));
+        std::vector<uint64_t> hpx, hpz;
+        const uint32_t nwt = L.nw_words;
+        if (K.out_final_px) {
+            hpx.resize(shots * nwt);
+            CUDA_OK(cudaMemcpyAsync(hpx.data(), K.out_final_px, hpx.size() * 8, cudaMemcpyDeviceToHost, st));
+        }
+        if (K.out_final_pz) {
+            hpz.resize(shots * nwt);
+            CUDA_OK(cudaMemcpyAsync(hpz.data(), K.out_final_pz, hpz.size() * 8, cudaMemcpyDeviceToHost, st));
+        }
+        CUDA_OK(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        const uint32_t nwo = std::max<uint32_t>(m.num_words, 1);
+        for (uint64_t s = 0; s < shots && !hpx.empty(); ++s)
+            for (uint32_t w = 0; w < nwo; ++w) out->final_px[s * nwo + w] = hpx[s * nwt + w];
+        for (uint64_t s = 0; s < shots && !hpz.empty(); ++s)
+            for (uint32_t w = 0; w < nwo; ++w) out->final_pz[s * nwo + w] = hpz[s * nwt + w];
+        const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
+        if (dev_err != 0) {
+            throw ApiError(CLIFFT_GPU_EDEVICE,
+                           dev_err == DEV_ERR_ZERO_NORM ? "active measurement on a zero-norm state"
+                                                        : "device reported an invalid opcode");
+        }
+        out->passed_shots = hs[2];
+        out->logical_errors = hs[3];
+        out->dust_clamps = hs[4];
+        if (out->observable_ones)
+            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[5 + i];
+        out->kernel_launches = 1;
+        out->kernel_ms = ms;
+        out->group_threads = L.warp ? 32u : uint32_t(L.threads);
+        out->state_in_smem = L.state_in_smem ? 1u : 0u;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+/*
+ * clifft_gpu.h -- C ABI of the B200 (sm_100a) Schrodinger-VM backend.
+ *
+ * The backend executes the reference compiler's bytecode unchanged: a program
+ * is handed over as a `clifft_program_image` (the flat form of
+ * clifft::CompiledModule, src/clifft/backend/backend.h:324-344), uploaded once,
+ * and then sampled in batches of shots by persistent CUDA kernels.
+ *
+ * Mapping onto the reference interface:
+ *   clifft_gpu_load          replaces handing a `const CompiledModule&` to the
+ *                            SVM (src/clifft/svm/svm.h:331,358); validates the
+ *                            bytecode against the executor's invariants
+ *                            (axis ranges, EXPAND on axis k, active measurement
+ *                            on axis k-1, pool indices) before anything runs;
+ *   clifft_gpu_sample        replaces clifft::sample (svm.h:331-332,
+ *                            src/clifft/svm/svm.cc:191-255) and, with
+ *                            CLIFFT_GPU_SURVIVORS, clifft::sample_survivors
+ *                            (svm.h:358-360, svm.cc:266-345); with
+ *                            CLIFFT_GPU_FORCED it is the batched form of the
+ *                            forced-outcome replay behind
+ *                            clifft::record_probabilities (svm.h:405-406,
+ *                            src/clifft/api/record_probabilities.cc:122-191)
+ *                            and of the forced-fault cursors of sample_k
+ *                            (svm.cc:497-520);
+ *   clifft_gpu_backend_name  mirrors clifft::svm_backend (svm.h:316);
+ *   clifft_gpu_last_error    carries the message the reference would throw
+ *                            (std::invalid_argument / std::runtime_error).
+ *
+ * Every entry point returns 0 on success or a negative status and never throws
+ * across the ABI. Calls are re-entrant: each call uses its own stream-ordered
+ * scratch, so concurrent host threads may sample the same program.
+ */
+#ifndef CLIFFT_GPU_H
+#define CLIFFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "clifft_program_image.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CLIFFT_GPU_OK 0
+#define CLIFFT_GPU_EINVAL (-1)   /* invalid argument / malformed bytecode (ValueError) */
+#define CLIFFT_GPU_ECUDA (-2)    /* CUDA runtime failure (RuntimeError) */
+#define CLIFFT_GPU_EDEVICE (-3)  /* kernel reported a device-side error (RuntimeError) */
+#define CLIFFT_GPU_ENOMEM (-4)   /* device allocation failed (MemoryError) */
+
+/* precision of the statevector (probability sums, gamma and renormalisation
+ * are always FP64) */
+#define CLIFFT_GPU_FP64 0u
+#define CLIFFT_GPU_FP32 1u
+
+/* sample flags */
+#define CLIFFT_GPU_SURVIVORS 0x01u      /* count survivors; shots stop at the first failing POSTSELECT */
+#define CLIFFT_GPU_FORCED_MEAS 0x02u    /* outcomes from forced_meas (record_probabilities semantics) */
+#define CLIFFT_GPU_FORCED_FAULTS 0x04u  /* fault sites / channels / readout flips from the CSR inputs */
+#define CLIFFT_GPU_DEVICE_PTRS 0x08u    /* every input/output pointer is a device pointer */
+#define CLIFFT_GPU_TRACE 0x10u          /* fill meas_prob and the final-state dump */
+
+typedef struct clifft_gpu_program clifft_gpu_program;
+
+typedef struct clifft_gpu_sample_args {
+    uint64_t shots;
+    uint64_t seed;          /* Philox key; shot s uses counter (draw/2, 0, first_shot + s) */
+    uint64_t first_shot;    /* global index of shot 0 (multi-GPU shards, resumption) */
+    uint32_t precision;     /* CLIFFT_GPU_FP64 or CLIFFT_GPU_FP32 */
+    uint32_t flags;
+    uint32_t group_threads; /* 0 = autotuned; 32 = one warp per shot; 64..1024 = one CTA per shot */
+    uint32_t reserved;
+    double dust_eps;        /* relative dust threshold; 0 = 1e-18 (FP64) / 1e-9 (FP32) */
+    /* CLIFFT_GPU_FORCED_MEAS: shots x total_meas_slots bytes (0/1) */
+    const uint8_t* forced_meas;
+    /* CLIFFT_GPU_FORCED_FAULTS: per-shot CSR over fired noise sites (ascending)
+     * with the fired channel (index within the site), and readout entries. */
+    const uint32_t* fault_offsets;   /* shots + 1 */
+    const uint32_t* fault_sites;
+    const uint32_t* fault_channels;
+    const uint32_t* readout_offsets; /* shots + 1 */
+    const uint32_t* readout_entries;
+    void* stream;                    /* cudaStream_t; NULL = the legacy default stream */
+} clifft_gpu_sample_args;
+
+typedef struct clifft_gpu_outputs {
+    /* Per-shot bit-packed records, little-endian bit order inside u64 words:
+     * bit i of row s is word[s * words + i / 64] >> (i % 64). Any may be NULL. */
+    uint64_t* meas;       /* shots x ceil(num_measurements / 64) */
+    uint64_t* det;        /* shots x ceil(num_detectors / 64) */
+    uint64_t* obs;        /* shots x ceil(num_observables / 64), XOR expected_observables */
+    double* exp_vals;     /* shots x num_exp_vals */
+    uint8_t* survived;    /* shots: 1 unless discarded by POSTSELECT / unreachable */
+    /* CLIFFT_GPU_TRACE */
+    double* meas_prob;    /* shots x total_meas_slots: probability of the realised outcome, NaN if not executed */
+    double* log_prob;     /* shots: forced-mode log probability (record_probabilities) */
+    uint32_t* final_k;    /* shots */
+    double* final_gamma;  /* shots x 2 */
+    uint64_t* final_px;   /* shots x num_words */
+    uint64_t* final_pz;
+    double* final_v;      /* dump_shots x 2^peak_rank x 2 (complex FP64) */
+    uint64_t dump_shots;  /* rows of final_v to fill (shots 0 .. dump_shots-1) */
+    /* host-side results (always host memory) */
+    uint64_t passed_shots;
+    uint64_t logical_errors;
+    uint64_t* observable_ones; /* num_observables counters, may be NULL */
+    uint64_t dust_clamps;
+    uint32_t kernel_launches;  /* kernels this call launched */
+    float kernel_ms;           /* device time of the sampling kernel(s) */
+    uint32_t group_threads;    /* shot-group size that ran */
+    uint32_t state_in_smem;    /* 1 if the statevectors lived in shared memory */
+} clifft_gpu_outputs;
+
+/* Upload + validate a program. *out receives an opaque handle. */
+int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out);
+/* Release a handle (waits for the device). */
+void clifft_gpu_free(clifft_gpu_program* prog);
+/* Sample. See the flags above for survivors / forced / trace behaviour. */
+int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
+                      clifft_gpu_outputs* out);
+/* "cuda:sm_100a" when a B200-class device is current; "unavailable:<why>" otherwise. */
+const char* clifft_gpu_backend_name(void);
+/* Message of the last failing call on this host thread. */
+const char* clifft_gpu_last_error(void);
+/* Program metadata accessors (host memory). */
+uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog);
+uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLIFFT_GPU_H */

@@ -231,8 +231,10 @@ def ref_time_sample(prog, shots: int, seed: int, threads: int, survivors: bool) 
 def ref_forced(prog, forced_meas: np.ndarray, faults=None, readout_faults=None) -> Dict[str, np.ndarray]:
     lib = ref_lib()
     slots = prog.total_meas_slots
-    fm = np.ascontiguousarray(forced_meas, dtype=np.uint8).reshape(-1, slots)
-    shots = fm.shape[0]
+    shots = int(np.shape(forced_meas)[0])
+    fm = np.ascontiguousarray(forced_meas, dtype=np.uint8).reshape(shots, slots)
+    if fm.size == 0:
+        fm = np.zeros((shots, 1), np.uint8)
     fo = fs = fc = ro = re_ = None
     if faults is not None:
         fo, fs = _csr([[f[0] for f in sh] for sh in faults])
