@@ -45,6 +45,7 @@ class Outputs(ctypes.Structure):
         ("final_px", P), ("final_pz", P), ("final_v", P), ("dump_shots", ctypes.c_uint64),
         ("passed_shots", ctypes.c_uint64), ("logical_errors", ctypes.c_uint64),
         ("observable_ones", P), ("dust_clamps", ctypes.c_uint64),
+        ("algorithmic_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_float),
         ("group_threads", ctypes.c_uint32), ("state_in_smem", ctypes.c_uint32),
     ]

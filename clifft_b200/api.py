@@ -107,7 +107,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
     if forced_meas is not None:
         fm = np.ascontiguousarray(forced_meas, np.uint8).reshape(shots, p.total_meas_slots)
         keep.append(fm)
-        a.forced_meas = fm.ctypes.data if fm.size else None
+        a.forced_meas = fm.ctypes.data if fm.size else None  # zero slots: nothing to force
         flags |= N.CLIFFT_GPU_FORCED_MEAS
     if faults is not None or readout_faults is not None:
         fo, fs = _csr([[f[0] for f in sh] for sh in faults] if faults is not None else None, shots)
@@ -156,6 +156,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         res["final_v"] = fv[..., 0] + 1j * fv[..., 1]
     res.update(passed_shots=int(o.passed_shots), logical_errors=int(o.logical_errors),
                observable_ones=ones[:p.num_observables].copy(), dust_clamps=int(o.dust_clamps),
+               algorithmic_bytes=int(o.algorithmic_bytes),
                kernel_ms=float(o.kernel_ms), kernel_launches=int(o.kernel_launches),
                group_threads=int(o.group_threads), state_in_smem=bool(o.state_in_smem))
     return res
@@ -163,7 +164,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
 
 def _stats(r) -> dict:
     return {k: r[k] for k in ("kernel_ms", "kernel_launches", "group_threads", "state_in_smem",
-                              "dust_clamps")}
+                              "dust_clamps", "algorithmic_bytes")}
 
 
 def sample(program: Program, shots: int, seed: Optional[int] = None, *,

@@ -526,12 +526,14 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const bool dev_ptrs = (args->flags & CLIFFT_GPU_DEVICE_PTRS) != 0;
         const bool forced_meas = (args->flags & CLIFFT_GPU_FORCED_MEAS) != 0;
         const bool forced_faults = (args->flags & CLIFFT_GPU_FORCED_FAULTS) != 0;
-        if (forced_meas && !args->forced_meas) invalid("CLIFFT_GPU_FORCED_MEAS needs forced_meas");
+        if (forced_meas && !args->forced_meas && m.total_meas_slots > 0)
+            invalid("CLIFFT_GPU_FORCED_MEAS needs forced_meas");
         if (forced_faults && (!args->fault_offsets || !args->readout_offsets))
             invalid("CLIFFT_GPU_FORCED_FAULTS needs fault_offsets and readout_offsets");
         out->passed_shots = 0;
         out->logical_errors = 0;
         out->dust_clamps = 0;
+        out->algorithmic_bytes = 0;
         out->kernel_launches = 0;
         out->kernel_ms = 0.f;
         if (shots == 0) return;
@@ -579,7 +581,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const size_t amp = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
         if (!L.state_in_smem)
             K.state_global = buf.alloc(size_t(L.blocks) * L.groups_per_block * L.state_stride * amp);
-        const size_t n_counters = 3 + m.num_observables;
+        const size_t n_counters = 4 + m.num_observables;
         auto* scratch = static_cast<unsigned long long*>(buf.alloc((2 + n_counters) * 8 + 64));
         CUDA_OK(cudaMemsetAsync(scratch, 0, (2 + n_counters) * 8 + 64, st));
         K.work_counter = scratch;
@@ -685,8 +687,9 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->passed_shots = hs[2];
         out->logical_errors = hs[3];
         out->dust_clamps = hs[4];
+        out->algorithmic_bytes = hs[5];
         if (out->observable_ones)
-            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[5 + i];
+            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[6 + i];
         out->kernel_launches = 1;
         out->kernel_ms = ms;
         out->group_threads = L.warp ? 32u : uint32_t(L.threads);

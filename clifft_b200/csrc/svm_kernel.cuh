@@ -85,7 +85,7 @@ struct KParams {
     uint64_t state_stride;  // amplitudes per group slab
     void* state_global;     // global slab base (when !state_in_smem)
     unsigned long long* work_counter;
-    unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3..] observable ones
+    unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3] algorithmic bytes, [4..] observable ones
     int* error_word;               // first device-side error code (0 = none)
     // forced inputs
     const uint8_t* forced_meas;
@@ -349,11 +349,15 @@ struct Shot {
     bool reachable;
     double log_prob;
     unsigned long long dust;
+    unsigned long long bytes;  // algorithmic statevector bytes moved by this shot
     const uint8_t* forced;
     double* meas_prob;
 
     __device__ Shot(const DevProg& p, const KParams& kp, T* vv, GroupShared s, uint64_t sh_idx)
         : P(p), K(kp), v(vv), sh(s), shot(sh_idx) {}
+
+    // algorithmic bytes of one sweep touching `amps` amplitudes (read + write counted separately)
+    __device__ __forceinline__ void account(uint64_t amps) { bytes += amps * sizeof(T); }
 
     __device__ __forceinline__ double uniform() { return philox_uniform(K.seed, K.first_shot + shot, draw++); }
 
@@ -388,6 +392,7 @@ struct Shot {
             uint64_t n = 1ull << k;
             for (uint64_t i = G::rank(); i < n; i += G::size()) v[i] = cscale(v[i], (R)g);
             G::sync();
+            account(2 * n);
             gamma.x /= g;
             gamma.y /= g;
         }
@@ -436,6 +441,7 @@ struct Shot {
             v[b0 | tb] = a;
         }
         G::sync();
+        account(1ull << k);
         frame_cnot(c, t);
     }
     // exec_array_cz (svm_kernels.inl:255-365)
@@ -446,6 +452,7 @@ struct Shot {
             v[idx] = cneg(v[idx]);
         }
         G::sync();
+        account(1ull << (k - 1));
         frame_cz(c, t);
     }
     // exec_array_swap (svm_kernels.inl:369-458)
@@ -458,6 +465,7 @@ struct Shot {
             v[base | bb] = x;
         }
         G::sync();
+        account(1ull << k);
         frame_swap(a, b);
     }
     // exec_array_multi_cnot (svm_kernels.inl:464-550)
@@ -472,6 +480,7 @@ struct Shot {
             }
         }
         G::sync();
+        account(1ull << k);
         for (uint32_t c = 0; c < k; ++c)
             if ((mask >> c) & 1ull) frame_cnot(c, t);
     }
@@ -483,6 +492,7 @@ struct Shot {
             if (__popcll(a & mask) & 1) v[a] = cneg(v[a]);
         }
         G::sync();
+        account(1ull << k);
         for (uint32_t t = 0; t < k; ++t)
             if ((mask >> t) & 1ull) frame_cz(c, t);
     }
@@ -497,6 +507,7 @@ struct Shot {
             v[i1] = cscale(csub(x, y), s);
         }
         G::sync();
+        account(2ull << k);
         frame_h(a);
     }
     // apply_phase_waterfall (svm_kernels.inl:764-830)
@@ -508,6 +519,7 @@ struct Shot {
             v[idx] = cmul(v[idx], ph);
         }
         G::sync();
+        account(1ull << k);
     }
     // exec_array_t / t_dag / rot (svm_kernels.inl:951-988,1044-1061)
     __device__ void array_rot(uint32_t a, double zr, double zi) {
@@ -535,6 +547,7 @@ struct Shot {
             for (uint64_t i = G::rank(); i < half; i += G::size()) v[half + i] = cmul(v[i], ph);
         }
         G::sync();
+        account(2ull << k);
         k++;
         scale_magnitude(CGPU_EXPAND_SCALE);
         if (with_phase && x) phase(make_double2(zr, zi));
@@ -559,6 +572,7 @@ struct Shot {
             v[i1] = cadd(cmul(m10, x), cmul(m11, y));
         }
         G::sync();
+        account(2ull << k);
     }
     // exec_array_u4 (svm_kernels.inl:1310-1531)
     __device__ void array_u4(uint32_t lo, uint32_t hi, uint32_t cp) {
@@ -593,6 +607,7 @@ struct Shot {
             v[b | lb | hb] = y[3];
         }
         G::sync();
+        account(2ull << k);
     }
 
     // ------------------------------------------------------- measurements
@@ -676,6 +691,7 @@ struct Shot {
             acc[1] += cnorm_d(v[i + half]);
         }
         group_reduce<G, 2>(acc, sh.red);
+        account(1ull << k);
         double p0 = acc[0], p1 = acc[1], total = p0 + p1;
         if (!(total > 0.0)) {
             if (G::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_ZERO_NORM);
@@ -696,6 +712,7 @@ struct Shot {
         if (b == 1) {
             for (uint64_t i = G::rank(); i < half; i += G::size()) v[i] = v[i + half];
             G::sync();
+            account(1ull << k);
         }
         k--;
         double pb = b ? p1 : p0;
@@ -730,6 +747,7 @@ struct Shot {
             acc[1] += cnorm_d(csub(x, y));
         }
         group_reduce<G, 2>(acc, sh.red);
+        account((1ull << k) * 2 + (1ull << (k - 1)));
         double pp = acc[0], pm = acc[1], total = pp + pm;
         if (!(total > 0.0)) {
             if (G::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_ZERO_NORM);
@@ -899,6 +917,7 @@ struct Shot {
                 acc[1] += br * ai + bi * ar;
             }
             group_reduce<G, 3>(acc, sh.red);
+            account(1ull << k);
             double2 num = dmul(make_double2(acc[0], acc[1]), iph);
             if (acc[2] > 0.0) result = num.x / acc[2];
             result = fmin(1.0, fmax(-1.0, result));
@@ -919,6 +938,7 @@ struct Shot {
         reachable = true;
         log_prob = 0.0;
         dust = 0;
+        bytes = 0;
         rec_dirty = false;
         forced = (K.flags & KF_FORCED_MEAS) ? K.forced_meas + shot * P.slots : nullptr;
         meas_prob = (K.flags & KF_TRACE) && K.out_meas_prob ? K.out_meas_prob + shot * P.slots : nullptr;
@@ -1089,11 +1109,12 @@ struct Shot {
                 for (uint32_t i = 0; i < P.num_obs; ++i)
                     if ((sh.obs[i >> 5] >> (i & 31)) & 1u) {
                         any = true;
-                        atomicAdd(K.counters + 3 + i, 1ull);
+                        atomicAdd(K.counters + 4 + i, 1ull);
                     }
                 if (any) atomicAdd(K.counters + 1, 1ull);
             }
             if (dust) atomicAdd(K.counters + 2, dust);
+            if (bytes) atomicAdd(K.counters + 3, bytes);
         }
         if (K.out_final_v && shot < K.dump_shots) {
             const uint64_t stride = 1ull << P.peak, n = 1ull << k;

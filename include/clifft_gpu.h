@@ -106,6 +106,7 @@ typedef struct clifft_gpu_outputs {
     uint64_t logical_errors;
     uint64_t* observable_ones; /* num_observables counters, may be NULL */
     uint64_t dust_clamps;
+    uint64_t algorithmic_bytes; /* statevector bytes the executed opcodes must move (read + write) */
     uint32_t kernel_launches;  /* kernels this call launched */
     float kernel_ms;           /* device time of the sampling kernel(s) */
     uint32_t group_threads;    /* shot-group size that ran */

@@ -19,7 +19,7 @@ from clifft_b200.program import (FLAG_EXPECTED_ONE, FLAG_IDENTITY, FLAG_SIGN, OP
 
 def random_program(seed: int, n: int = 10, length: int = 160, max_k: int = 6,
                    noise: bool = True, classical: bool = True, expvals: bool = True,
-                   postselect: bool = False, readout: bool = True) -> Program:
+                   postselect: bool = False, readout: bool = True, expand_bias: float = 0.12) -> Program:
     rng = np.random.default_rng(seed)
     W = (n + 63) // 64
     k = 0
@@ -48,7 +48,7 @@ def random_program(seed: int, n: int = 10, length: int = 160, max_k: int = 6,
 
     while len(code) < length:
         r = rng.random()
-        if r < 0.12 and k < max_k:
+        if (r < 0.12 or rng.random() < expand_bias - 0.12) and k < max_k:
             kind = rng.integers(0, 5)
             if rng.random() < 0.3:
                 emit(OP["FRAME_H"], k)

@@ -68,13 +68,15 @@ def main():
             s = O.ref_sample_survivors(prog, SAMPLE_SHOTS, seed, keep_records=True)
             d.update({f"surv_{k}": np.asarray(v) for k, v in s.items()})
         d["sample_seed"] = np.array(seed)
-        # forced inputs: outcomes from an oracle run (flip some to exercise
-        # unreachable records), random faults and readout flips
-        o = O.run(prog, FORCED_SHOTS, seed=seed + 1, rng=O.RNG_PHILOX)
+        # forced inputs: random faults and readout flips, and outcomes sampled
+        # by the oracle under those same faults (every 5th record flipped to
+        # exercise unreachable outcomes)
+        faults, ros = random_forced_inputs(prog, FORCED_SHOTS, seed + 2, fault_rate=0.2)
+        o = O.run(prog, FORCED_SHOTS, seed=seed + 1, rng=O.RNG_PHILOX, faults=faults,
+                  readout_faults=ros)
         fm = np.zeros((FORCED_SHOTS, prog.total_meas_slots), np.uint8)
         fm[:, :prog.num_measurements] = o["meas"]
         fm[::5] ^= 1
-        faults, ros = random_forced_inputs(prog, FORCED_SHOTS, seed + 2, fault_rate=0.2)
         f = O.ref_forced(prog, fm, faults, ros)
         d["forced_meas_in"] = fm
         fo = np.zeros(FORCED_SHOTS + 1, np.uint32)
@@ -98,6 +100,24 @@ def main():
               prog.peak_rank, prog.num_instructions)
 
 
+def bench_programs():
+    """Benchmark programs (reference bytecode passes applied) for bench.py:
+    programs/<name>.npz for configs 0, 1, 3 and the 64 programs of config 2."""
+    outdir = os.path.join(HERE, "programs")
+    os.makedirs(outdir, exist_ok=True)
+    items = [("cfg0", W.lower(W.config0())),
+             ("cfg1", W.lower(W.config1(), postselect_all=True)),
+             ("cfg3", W.lower(W.config3()))]
+    for i, c in enumerate(W.config2_circuits()):
+        items.append((f"cfg2_{i:02d}", W.lower(c)))
+    c4, theta = W.config4()
+    items.append(("cfg4", W.lower(c4)))
+    for name, raw in items:
+        prog = O.ref_passes(raw, O.PASS_ALL)
+        prog.name = name
+        prog.save(os.path.join(outdir, f"{name}.npz"))
+
+
 def load_case(path):
     """(program, dict of arrays) from a fixture file."""
     from clifft_b200.program import Program
@@ -119,3 +139,4 @@ def unflatten(d):
 
 if __name__ == "__main__":
     main()
+    bench_programs()
