@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libclifft_gpu.so")
 
-SOURCES = ["clifft_gpu.cu"]
-HEADERS = ["svm_kernel.cuh"]
+SOURCES = ["clifft_gpu.cu", "svm_kernels_f32.cu", "svm_kernels_f64.cu"]
+HEADERS = ["svm_kernel.cuh", "svm_dispatch.h", "svm_instantiate.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -54,11 +54,23 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", OUT + ".tmp"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(ROOT, "_build", "clifft_b200")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC]
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *flags, *inc, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((src, subprocess.Popen(cmd)))
+        objs.append(obj)
+    for src, pr in procs:
+        if pr.wait() != 0:
+            raise RuntimeError(f"nvcc failed on {src}")
+    subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs,
+                    "-o", OUT + ".tmp"], check=True)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "clifft_gpu.h"
+#include "svm_dispatch.h"
 #include "svm_kernel.cuh"
 
 using namespace cgpu;
@@ -266,26 +267,13 @@ const T* at(void* base, size_t off) {
     return reinterpret_cast<const T*>(static_cast<uint8_t*>(base) + off);
 }
 
-// kernel table ----------------------------------------------------------
-using KernelFn = void (*)(const DevProg, const KParams);
-
-template <typename R>
-KernelFn pick_kernel(bool warp, uint32_t nw) {
-    if (warp) {
-        if (nw <= 1) return svm_sample_kernel<R, WarpGroup, 1>;
-        if (nw <= 2) return svm_sample_kernel<R, WarpGroup, 2>;
-        return svm_sample_kernel<R, WarpGroup, 4>;
-    }
-    if (nw <= 1) return svm_sample_kernel<R, CtaGroup, 1>;
-    if (nw <= 2) return svm_sample_kernel<R, CtaGroup, 2>;
-    return svm_sample_kernel<R, CtaGroup, 4>;
-}
-
+// launch planning ---------------------------------------------------------
 struct LaunchPlan {
     KernelFn fn;
-    bool warp;
-    int threads;      // block size
-    int groups_per_block;
+    int G;             // lanes per shot (1..32), 0 = one CTA per shot
+    int S;             // shots per warp region (1 for CTA groups)
+    int threads;       // block size
+    int regions;       // warp regions (or 1 CTA region) per block
     int blocks;
     size_t smem;
     bool state_in_smem;
@@ -293,7 +281,17 @@ struct LaunchPlan {
     uint32_t nw_words;
 };
 
-uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : (nw <= 2 ? 2 : 4); }
+uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
+
+// Shot-group width for one warp: about 32 amplitudes per lane, so each warp
+// carries 32 / G shots whose statevectors interleave in 8 KiB (FP32) /
+// 16 KiB (FP64) of shared memory.
+int default_group(uint32_t peak) {
+    uint64_t amps = uint64_t(1) << peak;
+    int g = 1;
+    while (g < 32 && uint64_t(g) * 32 < amps) g <<= 1;
+    return g;
+}
 
 LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
                        uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words) {
@@ -301,67 +299,67 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const uint64_t stride = uint64_t(1) << p.meta.peak_rank;
     const size_t state_bytes = stride * amp;
-    const size_t rec_bytes = size_t(rec_words + det_words + obs_words) * 4;
     int dev = 0;
     CUDA_OK(cudaGetDevice(&dev));
     int smem_optin = 0, sms = 0;
     CUDA_OK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const size_t smem_cap = size_t(smem_optin) - 1024;
+    const size_t rec_bytes1 = size_t(rec_words + det_words + obs_words) * 4;
 
-    bool warp;
-    if (group_req == 32)
-        warp = true;
+    // group_req: 0 = heuristic; 1..32 = lanes per shot; 64..1024 = CTA of that size
+    int G;
+    if (group_req >= 1 && group_req <= 32)
+        G = int(group_req);
     else if (group_req > 32)
-        warp = false;
+        G = 0;
     else
-        warp = state_bytes <= 8192;  // k <= 10 (FP32) / k <= 9 (FP64): one warp per shot
-    L.warp = warp;
+        G = (state_bytes <= 16384) ? default_group(p.meta.peak_rank) : 0;
+    if (G != 0 && (G & (G - 1))) invalid("group_threads below 32 must be a power of two");
+    L.G = G;
+    L.S = G ? 32 / G : 1;
     L.nw_words = nw_template(p.meta.num_words);
-    L.fn = precision == CLIFFT_GPU_FP32 ? pick_kernel<float>(warp, L.nw_words)
-                                        : pick_kernel<double>(warp, L.nw_words);
+    L.fn = precision == CLIFFT_GPU_FP32 ? kernel_f32(G, int(L.nw_words)) : kernel_f64(G, int(L.nw_words));
     cudaFuncAttributes fa{};
     CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
     const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
-
-    if (warp) {
-        L.threads = std::min(256, max_threads);
-        L.groups_per_block = L.threads / 32;
-        size_t group = (state_bytes + rec_bytes + 15) & ~size_t(15);
-        // fall back to fewer warps per block if the slabs do not fit
-        while (L.groups_per_block > 1 &&
-               group * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64 > smem_cap) {
-            L.groups_per_block /= 2;
-            L.threads = L.groups_per_block * 32;
+    auto region_bytes = [&](bool in_smem) {
+        return ((in_smem ? state_bytes * L.S : 0) + rec_bytes1 * L.S + 15) & ~size_t(15);
+    };
+    auto tail = [&](int threads) { return size_t(3 * 8 * (threads / 32) + 64); };
+    if (G) {
+        L.threads = std::min(128, max_threads);
+        L.regions = L.threads / 32;
+        L.state_in_smem = region_bytes(true) + tail(32) <= smem_cap;
+        while (L.regions > 1 && region_bytes(L.state_in_smem) * L.regions + tail(L.threads) > smem_cap) {
+            L.regions /= 2;
+            L.threads = L.regions * 32;
         }
-        L.state_in_smem = group * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64 <= smem_cap;
     } else {
         int t = group_req > 32 ? int(group_req) : (state_bytes <= (size_t(32) << 10) ? 256 : 512);
-        if (!(group_req > 32) && state_bytes > (size_t(160) << 10)) t = 1024;
         L.threads = std::min(t, max_threads);
-        L.groups_per_block = 1;
-        size_t group = (state_bytes + rec_bytes + 15) & ~size_t(15);
-        L.state_in_smem = group + 3 * 8 * (L.threads / 32) + 64 <= smem_cap;
+        L.regions = 1;
+        L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
-    const size_t group_bytes =
-        ((L.state_in_smem ? state_bytes : 0) + rec_bytes + 15) & ~size_t(15);
-    L.smem = group_bytes * L.groups_per_block + 3 * 8 * (L.threads / 32) + 64;
+    L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
     CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(L.smem)));
     int per_sm = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)L.fn, L.threads, L.smem));
     if (per_sm < 1) invalid("kernel does not fit on an SM with this launch shape");
-    const uint64_t groups_needed = (shots + L.groups_per_block - 1) / L.groups_per_block;
+    const uint64_t shots_per_block = uint64_t(L.regions) * L.S;
+    const uint64_t blocks_needed = (shots + shots_per_block - 1) / shots_per_block;
     uint64_t blocks = uint64_t(per_sm) * sms;
     if (!L.state_in_smem) {
         // global slabs: bound the resident state to ~half of free HBM
         size_t free_b = 0, total_b = 0;
         CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
-        uint64_t max_groups = std::max<uint64_t>(1, (free_b / 2) / std::max<size_t>(state_bytes, 1));
-        blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, max_groups / L.groups_per_block));
+        uint64_t per_block_bytes = uint64_t(state_bytes) * shots_per_block;
+        uint64_t max_blocks = std::max<uint64_t>(1, (free_b / 2) / std::max<uint64_t>(per_block_bytes, 1));
+        blocks = std::min<uint64_t>(blocks, max_blocks);
     }
-    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, groups_needed));
+    blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, blocks_needed));
     L.blocks = int(blocks);
     L.state_stride = stride;
     return L;
@@ -580,7 +578,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         K.state_stride = L.state_stride;
         const size_t amp = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
         if (!L.state_in_smem)
-            K.state_global = buf.alloc(size_t(L.blocks) * L.groups_per_block * L.state_stride * amp);
+            K.state_global = buf.alloc(size_t(L.blocks) * L.regions * L.S * L.state_stride * amp);
         const size_t n_counters = 4 + m.num_observables;
         auto* scratch = static_cast<unsigned long long*>(buf.alloc((2 + n_counters) * 8 + 64));
         CUDA_OK(cudaMemsetAsync(scratch, 0, (2 + n_counters) * 8 + 64, st));
@@ -692,7 +690,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
             for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[6 + i];
         out->kernel_launches = 1;
         out->kernel_ms = ms;
-        out->group_threads = L.warp ? 32u : uint32_t(L.threads);
+        out->group_threads = L.G ? uint32_t(L.G) : uint32_t(L.threads);
         out->state_in_smem = L.state_in_smem ? 1u : 0u;
     });
 }

@@ -1,22 +1,34 @@
 // svm_kernel.cuh -- persistent shot-parallel Schrodinger-VM interpreter for sm_100a.
 //
-// One *shot group* (a warp, or a whole CTA) runs one shot of the reference's
-// bytecode at a time and pulls the next shot index from a global work counter
-// as soon as it finishes, so shots that die early (post-selection, unreachable
-// forced outcomes) are replaced immediately (work-queue compaction).
+// Work decomposition. A *shot group* of G lanes runs one shot of the
+// reference's bytecode:
+//   * G in {1, 2, 4, 8, 16, 32}: a warp carries S = 32 / G shots side by side
+//     and walks the (shared, read-only) instruction stream in lockstep, so one
+//     issued instruction advances S shots. Frame opcodes, noise, records and
+//     detector logic cost one lane-instruction per shot instead of 32;
+//     statevector sweeps are split over the G lanes of each shot. A warp takes
+//     S shot indices at a time from a global work counter; a shot that stops
+//     early (post-selection, unreachable forced outcome) parks its lanes until
+//     the warp's other shots finish.
+//   * G = 0: a whole CTA runs one shot (large k); sweeps use every thread and
+//     the shot index comes from the work counter, so the CTA moves on as soon as
+//     its shot ends.
+// Statevectors live in shared memory when they fit and otherwise in a global
+// slab per warp / CTA. Within a warp the S statevectors are interleaved
+// (amplitude i of shot slot s at [i * S + s]) so lanes of different shots
+// touching the same amplitude index hit consecutive banks / addresses.
 //
 // Per shot, the factored state |psi> = gamma * U_C * P * (|phi>_A (x) |0>_D)
 // (src/clifft/svm/svm.h:92-103) is held as:
-//   * the 2^k active amplitudes in shared memory (small k) or in a per-group
-//     global slab (large k), complex FP32 or FP64;
-//   * the Pauli frame p_x / p_z as NW 64-bit words in registers of every thread
-//     of the group (updated redundantly, so frame opcodes cost no barrier);
+//   * the 2^k active amplitudes, complex FP32 or FP64;
+//   * the Pauli frame p_x / p_z as NW 64-bit words in registers of every lane
+//     of the group (updated redundantly: frame opcodes need no barrier);
 //   * gamma as an FP64 complex in registers;
 //   * measurement / detector / observable records as bit arrays in shared
 //     memory.
 // Branch probabilities and expectation values are reduced in FP64 with a fixed
-// summation order, so every thread of the group derives the same outcome from
-// the same counter-based Philox draw (identical control flow, no broadcast).
+// summation order, so every lane of a group derives the same outcome from the
+// same counter-based Philox draw (identical control flow, no broadcast).
 //
 // Opcode semantics follow the reference kernels in
 // src/clifft/svm/svm_kernels.inl and svm_forced_kernels.cc; each handler cites
@@ -75,15 +87,15 @@ struct KParams {
     uint64_t seed;
     double dust_eps;
     uint32_t flags;
-    uint32_t rec_words;   // u32 words of measurement record per group (>= ceil(slots/32))
-    uint32_t det_words;   // u32 words of detector record
-    uint32_t obs_words;   // u32 words of observable record
+    uint32_t rec_words;       // u32 words of measurement record per shot (>= ceil(slots/32))
+    uint32_t det_words;       // u32 words of detector record per shot
+    uint32_t obs_words;       // u32 words of observable record per shot
     uint32_t meas_out_words;  // u64 words per shot in outputs
     uint32_t det_out_words;
     uint32_t obs_out_words;
     uint32_t state_in_smem;
-    uint64_t state_stride;  // amplitudes per group slab
-    void* state_global;     // global slab base (when !state_in_smem)
+    uint64_t state_stride;    // amplitudes per shot slot (2^peak_rank)
+    void* state_global;       // global slab base (when !state_in_smem)
     unsigned long long* work_counter;
     unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3] algorithmic bytes, [4..] observable ones
     int* error_word;               // first device-side error code (0 = none)
@@ -215,21 +227,38 @@ __device__ __forceinline__ double philox_uniform(uint64_t seed, uint64_t shot, u
 }
 
 // ------------------------------------------------------------------ groups
-struct WarpGroup {
-    static constexpr bool kIsWarp = true;
-    __device__ static __forceinline__ int size() { return 32; }
-    __device__ static __forceinline__ int rank() { return threadIdx.x & 31; }
-    __device__ static __forceinline__ int local() { return threadIdx.x >> 5; }
-    __device__ static __forceinline__ int per_block() { return blockDim.x >> 5; }
-    __device__ static __forceinline__ void sync() { __syncwarp(); }
+// G lanes of one warp per shot (G = 1..32), S = 32 / G shots per warp.
+template <int G>
+struct Lanes {
+    static constexpr bool kCta = false;
+    static constexpr int S = 32 / G;
+    __device__ static __forceinline__ int size() { return G; }
+    __device__ static __forceinline__ int rank() { return (int)(threadIdx.x & 31) & (G - 1); }
+    __device__ static __forceinline__ int slot() { return (int)(threadIdx.x & 31) / G; }
+    __device__ static __forceinline__ unsigned mask() {
+        return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(unsigned)(G - 1)));
+    }
+    __device__ static __forceinline__ void sync() {
+        if (G > 1) __syncwarp(mask());
+    }
 };
-struct CtaGroup {
-    static constexpr bool kIsWarp = false;
+// A whole CTA per shot.
+struct CtaLanes {
+    static constexpr bool kCta = true;
+    static constexpr int S = 1;
     __device__ static __forceinline__ int size() { return blockDim.x; }
     __device__ static __forceinline__ int rank() { return threadIdx.x; }
-    __device__ static __forceinline__ int local() { return 0; }
-    __device__ static __forceinline__ int per_block() { return 1; }
+    __device__ static __forceinline__ int slot() { return 0; }
+    __device__ static __forceinline__ unsigned mask() { return 0xffffffffu; }
     __device__ static __forceinline__ void sync() { __syncthreads(); }
+};
+template <int G>
+struct GroupOf {
+    using type = Lanes<G>;
+};
+template <>
+struct GroupOf<0> {
+    using type = CtaLanes;
 };
 
 __device__ __forceinline__ uint64_t ins0(uint64_t v, uint32_t pos) {
@@ -261,45 +290,42 @@ struct Frame {
     __device__ static __forceinline__ void put(uint64_t* w, uint32_t a, int b) {
 #pragma unroll
         for (int i = 0; i < NW; ++i)
-            if ((uint32_t)i == (a >> 6)) {
+            if (NW == 1 || (uint32_t)i == (a >> 6)) {
                 uint64_t m = 1ull << (a & 63);
                 w[i] = b ? (w[i] | m) : (w[i] & ~m);
             }
     }
     __device__ static __forceinline__ void flip(uint64_t* w, uint32_t a, int b) {
-        if (b) {
 #pragma unroll
-            for (int i = 0; i < NW; ++i)
-                if ((uint32_t)i == (a >> 6)) w[i] ^= 1ull << (a & 63);
-        }
+        for (int i = 0; i < NW; ++i)
+            if (NW == 1 || (uint32_t)i == (a >> 6)) w[i] ^= (uint64_t)(b & 1) << (a & 63);
     }
     __device__ __forceinline__ int px(uint32_t a) const { return get(x, a); }
     __device__ __forceinline__ int pz(uint32_t a) const { return get(z, a); }
 };
 
-// Shared per-group scratch.
-struct GroupShared {
-    uint32_t* rec;     // rec_words
-    uint32_t* det;     // det_words
-    uint32_t* obs;     // obs_words
-    double* red;       // reduction scratch: 3 * warps
-    unsigned long long* bcast;
-};
-
-// FP64 group reduction of N values with a fixed order: warp tree to lane 0,
-// warps combined in index order by every thread. All threads return the same
-// bits.
-template <class G, int N>
+// FP64 reduction of N values over one shot group with a fixed order (lane
+// tree within the group, then warps in index order for a CTA). Every lane of
+// the group returns the same bits.
+template <class Grp, int N>
 __device__ __forceinline__ void group_reduce(double (&v)[N], double* red) {
+    if (!Grp::kCta) {
+        constexpr int G = 32 / Grp::S;
+        if (G > 1) {
+            const unsigned m = Grp::mask();
+#pragma unroll
+            for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+                for (int j = 0; j < N; ++j) v[j] += __shfl_down_sync(m, v[j], off, G);
+#pragma unroll
+            for (int j = 0; j < N; ++j) v[j] = __shfl_sync(m, v[j], 0, G);
+        }
+        return;
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
 #pragma unroll
         for (int j = 0; j < N; ++j) v[j] += __shfl_down_sync(0xffffffffu, v[j], off);
-    if (G::kIsWarp) {
-#pragma unroll
-        for (int j = 0; j < N; ++j) v[j] = __shfl_sync(0xffffffffu, v[j], 0);
-        return;
-    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     if (lane == 0)
 #pragma unroll
@@ -313,29 +339,27 @@ __device__ __forceinline__ void group_reduce(double (&v)[N], double* red) {
     __syncthreads();
 }
 
-template <class G>
-__device__ __forceinline__ unsigned long long group_next_shot(unsigned long long* counter,
-                                                              unsigned long long* bcast) {
-    unsigned long long s = 0;
-    if (G::rank() == 0) s = atomicAdd(counter, 1ull);
-    if (G::kIsWarp) return __shfl_sync(0xffffffffu, s, 0);
-    if (G::rank() == 0) *bcast = s;
-    __syncthreads();
-    s = *bcast;
-    __syncthreads();
-    return s;
+__device__ __forceinline__ int bit_of(const uint32_t* r, uint32_t i, int S) {
+    return (int)((r[(i >> 5) * S] >> (i & 31)) & 1u);
 }
 
-__device__ __forceinline__ int rec_get(const uint32_t* r, uint32_t i) { return (int)((r[i >> 5] >> (i & 31)) & 1u); }
+// Per-lane totals flushed once per kernel.
+struct Tally {
+    unsigned long long passed = 0, logical = 0, dust = 0, bytes = 0;
+};
 
 // --------------------------------------------------------------- the shot
-template <typename R, class G, int NW>
+template <typename R, class Grp, int NW>
 struct Shot {
     using T = typename Cx<R>::T;
+    static constexpr int S = Grp::S;
     const DevProg& P;
     const KParams& K;
-    T* v;
-    GroupShared sh;
+    T* v;           // slot base: amplitude i at v[i * S]
+    uint32_t* rec;  // record words: word w at rec[w * S]
+    uint32_t* det;
+    uint32_t* obs;
+    double* red;
     uint64_t shot;
     Frame<NW> f;
     double2 gamma;
@@ -353,27 +377,27 @@ struct Shot {
     const uint8_t* forced;
     double* meas_prob;
 
-    __device__ Shot(const DevProg& p, const KParams& kp, T* vv, GroupShared s, uint64_t sh_idx)
-        : P(p), K(kp), v(vv), sh(s), shot(sh_idx) {}
+    __device__ __forceinline__ Shot(const DevProg& p, const KParams& kp, T* vv, uint32_t* r, uint32_t* d,
+                                    uint32_t* o, double* rd, uint64_t s)
+        : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s) {}
 
-    // algorithmic bytes of one sweep touching `amps` amplitudes (read + write counted separately)
+    __device__ __forceinline__ T& A(uint64_t i) { return v[i * S]; }
     __device__ __forceinline__ void account(uint64_t amps) { bytes += amps * sizeof(T); }
-
     __device__ __forceinline__ double uniform() { return philox_uniform(K.seed, K.first_shot + shot, draw++); }
-
     __device__ __forceinline__ void phase(double2 p) { gamma = dmul(gamma, p); }
     __device__ __forceinline__ void negate_gamma() { gamma = make_double2(-gamma.x, -gamma.y); }
 
     __device__ __forceinline__ void flush_records() {
         if (rec_dirty) {
-            G::sync();
+            Grp::sync();
             rec_dirty = false;
         }
     }
     __device__ __forceinline__ void write_meas(uint32_t idx, int bit, double prob) {
-        if (G::rank() == 0) {
+        if (Grp::rank() == 0) {
             uint32_t m = 1u << (idx & 31);
-            sh.rec[idx >> 5] = bit ? (sh.rec[idx >> 5] | m) : (sh.rec[idx >> 5] & ~m);
+            uint32_t& w = rec[(idx >> 5) * S];
+            w = bit ? (w | m) : (w & ~m);
             if (meas_prob) meas_prob[idx] = prob;
         }
         rec_dirty = true;
@@ -382,7 +406,7 @@ struct Shot {
     // SchrodingerState::scale_magnitude (src/clifft/svm/svm.h:177-186). The
     // lazy-renormalisation window is 1e+-100 in FP64 and 1e+-20 in FP32 so the
     // FP32 amplitudes never approach their exponent range.
-    __device__ void scale_magnitude(double s) {
+    __device__ __forceinline__ void scale_magnitude(double s) {
         gamma.x *= s;
         gamma.y *= s;
         const double hi = sizeof(R) == 8 ? 1e100 : 1e20;
@@ -390,8 +414,8 @@ struct Shot {
         double g = hypot(gamma.x, gamma.y);
         if (g > hi || (g < lo && g > 0.0)) {
             uint64_t n = 1ull << k;
-            for (uint64_t i = G::rank(); i < n; i += G::size()) v[i] = cscale(v[i], (R)g);
-            G::sync();
+            for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) A(i) = cscale(A(i), (R)g);
+            Grp::sync();
             account(2 * n);
             gamma.x /= g;
             gamma.y /= g;
@@ -432,97 +456,97 @@ struct Shot {
 
     // ---------------------------------------------------------- array ops
     // exec_array_cnot (svm_kernels.inl:124-252)
-    __device__ void array_cnot(uint32_t c, uint32_t t) {
+    __device__ __forceinline__ void array_cnot(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), cb = 1ull << c, tb = 1ull << t;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t b0 = ins00(i, c, t) | cb;
-            T a = v[b0], b = v[b0 | tb];
-            v[b0] = b;
-            v[b0 | tb] = a;
+            T a = A(b0), b = A(b0 | tb);
+            A(b0) = b;
+            A(b0 | tb) = a;
         }
-        G::sync();
+        Grp::sync();
         account(1ull << k);
         frame_cnot(c, t);
     }
     // exec_array_cz (svm_kernels.inl:255-365)
-    __device__ void array_cz(uint32_t c, uint32_t t) {
+    __device__ __forceinline__ void array_cz(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), both = (1ull << c) | (1ull << t);
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t idx = ins00(i, c, t) | both;
-            v[idx] = cneg(v[idx]);
+            A(idx) = cneg(A(idx));
         }
-        G::sync();
+        Grp::sync();
         account(1ull << (k - 1));
         frame_cz(c, t);
     }
     // exec_array_swap (svm_kernels.inl:369-458)
-    __device__ void array_swap(uint32_t a, uint32_t b) {
+    __device__ __forceinline__ void array_swap(uint32_t a, uint32_t b) {
         const uint64_t n = 1ull << (k - 2), ab = 1ull << a, bb = 1ull << b;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t base = ins00(i, a, b);
-            T x = v[base | ab], y = v[base | bb];
-            v[base | ab] = y;
-            v[base | bb] = x;
+            T x = A(base | ab), y = A(base | bb);
+            A(base | ab) = y;
+            A(base | bb) = x;
         }
-        G::sync();
+        Grp::sync();
         account(1ull << k);
         frame_swap(a, b);
     }
     // exec_array_multi_cnot (svm_kernels.inl:464-550)
-    __device__ void array_multi_cnot(uint32_t t, uint64_t mask) {
+    __device__ __forceinline__ void array_multi_cnot(uint32_t t, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), tb = 1ull << t;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t a = ins0(i, t);
             if (__popcll(a & mask) & 1) {
-                T x = v[a], y = v[a | tb];
-                v[a] = y;
-                v[a | tb] = x;
+                T x = A(a), y = A(a | tb);
+                A(a) = y;
+                A(a | tb) = x;
             }
         }
-        G::sync();
+        Grp::sync();
         account(1ull << k);
         for (uint32_t c = 0; c < k; ++c)
             if ((mask >> c) & 1ull) frame_cnot(c, t);
     }
     // exec_array_multi_cz (svm_kernels.inl:558-635)
-    __device__ void array_multi_cz(uint32_t c, uint64_t mask) {
+    __device__ __forceinline__ void array_multi_cz(uint32_t c, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), cb = 1ull << c;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t a = ins0(i, c) | cb;
-            if (__popcll(a & mask) & 1) v[a] = cneg(v[a]);
+            if (__popcll(a & mask) & 1) A(a) = cneg(A(a));
         }
-        G::sync();
+        Grp::sync();
         account(1ull << k);
         for (uint32_t t = 0; t < k; ++t)
             if ((mask >> t) & 1ull) frame_cz(c, t);
     }
     // exec_array_h (svm_kernels.inl:639-744)
-    __device__ void array_h(uint32_t a) {
+    __device__ __forceinline__ void array_h(uint32_t a) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const R s = (R)CGPU_INV_SQRT2;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t i0 = ins0(i, a), i1 = i0 | ab;
-            T x = v[i0], y = v[i1];
-            v[i0] = cscale(cadd(x, y), s);
-            v[i1] = cscale(csub(x, y), s);
+            T x = A(i0), y = A(i1);
+            A(i0) = cscale(cadd(x, y), s);
+            A(i1) = cscale(csub(x, y), s);
         }
-        G::sync();
+        Grp::sync();
         account(2ull << k);
         frame_h(a);
     }
     // apply_phase_waterfall (svm_kernels.inl:764-830)
-    __device__ void phase_sweep(uint32_t a, double re, double im) {
+    __device__ __forceinline__ void phase_sweep(uint32_t a, double re, double im) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const T ph = Cx<R>::make(re, im);
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t idx = ins0(i, a) | ab;
-            v[idx] = cmul(v[idx], ph);
+            A(idx) = cmul(A(idx), ph);
         }
-        G::sync();
+        Grp::sync();
         account(1ull << k);
     }
     // exec_array_t / t_dag / rot (svm_kernels.inl:951-988,1044-1061)
-    __device__ void array_rot(uint32_t a, double zr, double zi) {
+    __device__ __forceinline__ void array_rot(uint32_t a, double zr, double zi) {
         int x = f.px(a);
         if (a >= k) {
             if (x) phase(make_double2(zr, zi));
@@ -537,23 +561,23 @@ struct Shot {
     }
     // exec_expand / expand_with_phase / exec_expand_{t,t_dag,rot}
     // (svm_kernels.inl:876-1081)
-    __device__ void expand(uint32_t a, bool with_phase, double zr, double zi) {
+    __device__ __forceinline__ void expand(uint32_t a, bool with_phase, double zr, double zi) {
         const uint64_t half = 1ull << k;
         int x = with_phase ? f.px(a) : 0;
         if (!with_phase) {
-            for (uint64_t i = G::rank(); i < half; i += G::size()) v[half + i] = v[i];
+            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(half + i) = A(i);
         } else {
             const T ph = Cx<R>::make(zr, x ? -zi : zi);
-            for (uint64_t i = G::rank(); i < half; i += G::size()) v[half + i] = cmul(v[i], ph);
+            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(half + i) = cmul(A(i), ph);
         }
-        G::sync();
+        Grp::sync();
         account(2ull << k);
         k++;
         scale_magnitude(CGPU_EXPAND_SCALE);
         if (with_phase && x) phase(make_double2(zr, zi));
     }
     // exec_array_u2 (svm_kernels.inl:1087-1297)
-    __device__ void array_u2(uint32_t a, uint32_t cp) {
+    __device__ __forceinline__ void array_u2(uint32_t a, uint32_t cp) {
         const double* node = P.u2 + (size_t)cp * CLIFFT_U2_DOUBLES_PER_NODE;
         int st = (f.pz(a) << 1) | f.px(a);
         const double* m = node + st * 10;
@@ -565,17 +589,17 @@ struct Shot {
         const T m00 = Cx<R>::make(m[0], m[1]), m01 = Cx<R>::make(m[2], m[3]);
         const T m10 = Cx<R>::make(m[4], m[5]), m11 = Cx<R>::make(m[6], m[7]);
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t i0 = ins0(i, a), i1 = i0 | ab;
-            T x = v[i0], y = v[i1];
-            v[i0] = cadd(cmul(m00, x), cmul(m01, y));
-            v[i1] = cadd(cmul(m10, x), cmul(m11, y));
+            T x = A(i0), y = A(i1);
+            A(i0) = cadd(cmul(m00, x), cmul(m01, y));
+            A(i1) = cadd(cmul(m10, x), cmul(m11, y));
         }
-        G::sync();
+        Grp::sync();
         account(2ull << k);
     }
     // exec_array_u4 (svm_kernels.inl:1310-1531)
-    __device__ void array_u4(uint32_t lo, uint32_t hi, uint32_t cp) {
+    __device__ __forceinline__ void array_u4(uint32_t lo, uint32_t hi, uint32_t cp) {
         const double* node = P.u4 + (size_t)cp * CLIFFT_U4_DOUBLES_PER_NODE;
         int st = (f.pz(hi) << 3) | (f.px(hi) << 2) | (f.pz(lo) << 1) | f.px(lo);
         const double* e = node + st * 34;
@@ -585,28 +609,26 @@ struct Shot {
         Frame<NW>::put(f.z, lo, (out >> 1) & 1);
         Frame<NW>::put(f.x, hi, (out >> 2) & 1);
         Frame<NW>::put(f.z, hi, (out >> 3) & 1);
-        T m[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) m[j] = Cx<R>::make(e[2 * j], e[2 * j + 1]);
         const uint64_t n = 1ull << (k - 2), lb = 1ull << lo, hb = 1ull << hi;
-        for (uint64_t i = G::rank(); i < n; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
             uint64_t b = ins00(i, lo, hi);
-            T x0 = v[b], x1 = v[b | lb], x2 = v[b | hb], x3 = v[b | lb | hb];
+            T x0 = A(b), x1 = A(b | lb), x2 = A(b | hb), x3 = A(b | lb | hb);
             T y[4];
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                T acc = cmul(m[r * 4 + 0], x0);
-                acc = cadd(acc, cmul(m[r * 4 + 1], x1));
-                acc = cadd(acc, cmul(m[r * 4 + 2], x2));
-                acc = cadd(acc, cmul(m[r * 4 + 3], x3));
+                const double* row = e + r * 8;
+                T acc = cmul(Cx<R>::make(row[0], row[1]), x0);
+                acc = cadd(acc, cmul(Cx<R>::make(row[2], row[3]), x1));
+                acc = cadd(acc, cmul(Cx<R>::make(row[4], row[5]), x2));
+                acc = cadd(acc, cmul(Cx<R>::make(row[6], row[7]), x3));
                 y[r] = acc;
             }
-            v[b] = y[0];
-            v[b | lb] = y[1];
-            v[b | hb] = y[2];
-            v[b | lb | hb] = y[3];
+            A(b) = y[0];
+            A(b | lb) = y[1];
+            A(b | hb) = y[2];
+            A(b | lb | hb) = y[3];
         }
-        G::sync();
+        Grp::sync();
         account(2ull << k);
     }
 
@@ -616,33 +638,23 @@ struct Shot {
     // (src/clifft/svm/svm_forced_kernels.cc:42-60). `want` is the forced
     // branch or -1. Returns the branch, or -1 when the forced branch is
     // unreachable.
-    __device__ int choose(double p0, double p1, double total, int want, double* prob) {
+    __device__ __forceinline__ int choose(double p0, double p1, double total, int want, double* prob) {
         const double eps = K.dust_eps * total;
-        if (want < 0) {
-            if (p1 <= eps) {
-                if (p1 > 0.0) dust++;
-                *prob = 1.0;
-                return 0;
-            }
-            if (p0 <= eps) {
-                if (p0 > 0.0) dust++;
-                *prob = 1.0;
-                return 1;
-            }
-            double r = uniform();
-            int b = (r * total < p0) ? 0 : 1;
-            *prob = (b ? p1 : p0) / total;
-            return b;
-        }
         if (p1 <= eps) {
             if (p1 > 0.0) dust++;
             *prob = 1.0;
-            return want == 0 ? 0 : -1;
+            return want <= 0 ? 0 : -1;
         }
         if (p0 <= eps) {
             if (p0 > 0.0) dust++;
             *prob = 1.0;
-            return want == 1 ? 1 : -1;
+            return (want < 0 || want == 1) ? 1 : -1;
+        }
+        if (want < 0) {
+            double r = uniform();
+            int b = (r * total < p0) ? 0 : 1;
+            *prob = (b ? p1 : p0) / total;
+            return b;
         }
         double pb = (want ? p1 : p0) / total;
         log_prob += log(pb);
@@ -654,19 +666,19 @@ struct Shot {
 
     // exec_meas_dormant_static + FLAG_IDENTITY shortcut (svm_kernels.inl:1539-1545,
     // 2361-2369) and forced variants (svm_forced_kernels.cc:64-88)
-    __device__ void meas_dormant_static(uint32_t a, uint32_t idx, int sign, bool identity) {
-        int det = identity ? sign : (f.px(a) ^ sign);
+    __device__ __forceinline__ void meas_dormant_static(uint32_t a, uint32_t idx, int sign, bool identity) {
+        int det_bit = identity ? sign : (f.px(a) ^ sign);
         int want = forced_bit(idx);
-        if (want >= 0 && want != det) {
+        if (want >= 0 && want != det_bit) {
             reachable = false;
             stop = true;
             return;
         }
-        write_meas(idx, det, 1.0);
+        write_meas(idx, det_bit, 1.0);
     }
     // exec_meas_dormant_random (svm_kernels.inl:1550-1566), forced
     // (svm_forced_kernels.cc:90-110)
-    __device__ void meas_dormant_random(uint32_t a, uint32_t idx, int sign) {
+    __device__ __forceinline__ void meas_dormant_random(uint32_t a, uint32_t idx, int sign) {
         int want = forced_bit(idx);
         int m_abs;
         if (want >= 0) {
@@ -680,24 +692,28 @@ struct Shot {
         Frame<NW>::put(f.z, a, 0);
         write_meas(idx, m_abs ^ sign, 0.5);
     }
+    __device__ __forceinline__ bool zero_norm(double total) {
+        if (!(total > 0.0)) {
+            if (Grp::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_ZERO_NORM);
+            stop = true;
+            return true;
+        }
+        return false;
+    }
     // exec_meas_active_diagonal (svm_kernels.inl:1573-1627), forced
     // (svm_forced_kernels.cc:112-158)
-    __device__ void meas_diagonal(uint32_t a, uint32_t idx, int sign) {
+    __device__ __forceinline__ void meas_diagonal(uint32_t a, uint32_t idx, int sign) {
         const uint64_t half = 1ull << (k - 1);
         int pxv = f.px(a), pzv = f.pz(a);
         double acc[2] = {0.0, 0.0};
-        for (uint64_t i = G::rank(); i < half; i += G::size()) {
-            acc[0] += cnorm_d(v[i]);
-            acc[1] += cnorm_d(v[i + half]);
+        for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
+            acc[0] += cnorm_d(A(i));
+            acc[1] += cnorm_d(A(i + half));
         }
-        group_reduce<G, 2>(acc, sh.red);
+        group_reduce<Grp, 2>(acc, red);
         account(1ull << k);
         double p0 = acc[0], p1 = acc[1], total = p0 + p1;
-        if (!(total > 0.0)) {
-            if (G::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_ZERO_NORM);
-            stop = true;
-            return;
-        }
+        if (zero_norm(total)) return;
         int want = forced_bit(idx);
         if (want >= 0) want = want ^ sign ^ pxv;
         double prob;
@@ -710,8 +726,8 @@ struct Shot {
         int m_abs = b ^ pxv;
         if (b == 1 && pzv) negate_gamma();
         if (b == 1) {
-            for (uint64_t i = G::rank(); i < half; i += G::size()) v[i] = v[i + half];
-            G::sync();
+            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(i) = A(i + half);
+            Grp::sync();
             account(1ull << k);
         }
         k--;
@@ -727,13 +743,13 @@ struct Shot {
     // the fold runs in two passes over disjoint outputs (bit f clear, then
     // set) because the f-clear outputs read lower-half inputs that f-set
     // outputs overwrite; the reference serialises this loop instead.
-    __device__ void meas_interfere(uint32_t fa, uint32_t t, uint32_t idx, int sign) {
+    __device__ __forceinline__ void meas_interfere(uint32_t fa, uint32_t t, uint32_t idx, int sign) {
         const bool swapped = fa != t;
         if (swapped) frame_swap(fa, t);
         int pxv = f.px(t), pzv = f.pz(t);
         const uint64_t half = 1ull << t, fb = 1ull << fa;
         double acc[2] = {0.0, 0.0};
-        for (uint64_t i = G::rank(); i < half; i += G::size()) {
+        for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
             uint64_t a0, a1;
             if (swapped) {
                 a0 = (i & ~fb) | (((i >> fa) & 1ull) << t);
@@ -742,18 +758,14 @@ struct Shot {
                 a0 = i;
                 a1 = i + half;
             }
-            T x = v[a0], y = v[a1];
+            T x = A(a0), y = A(a1);
             acc[0] += cnorm_d(cadd(x, y));
             acc[1] += cnorm_d(csub(x, y));
         }
-        group_reduce<G, 2>(acc, sh.red);
+        group_reduce<Grp, 2>(acc, red);
         account((1ull << k) * 2 + (1ull << (k - 1)));
         double pp = acc[0], pm = acc[1], total = pp + pm;
-        if (!(total > 0.0)) {
-            if (G::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_ZERO_NORM);
-            stop = true;
-            return;
-        }
+        if (zero_norm(total)) return;
         int want = forced_bit(idx);
         if (want >= 0) want = want ^ sign ^ pzv;
         double prob;
@@ -766,22 +778,22 @@ struct Shot {
         int m_abs = bx ^ pzv;
         const R s = (R)CGPU_INV_SQRT2;
         if (!swapped) {
-            for (uint64_t i = G::rank(); i < half; i += G::size()) {
-                T x = v[i], y = v[i + half];
-                v[i] = cscale(bx ? csub(x, y) : cadd(x, y), s);
+            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
+                T x = A(i), y = A(i + half);
+                A(i) = cscale(bx ? csub(x, y) : cadd(x, y), s);
             }
-            G::sync();
+            Grp::sync();
         } else {
             const uint64_t q = half >> 1;  // outputs with bit fa clear, then set
             for (int pass = 0; pass < 2; ++pass) {
-                for (uint64_t j = G::rank(); j < q; j += G::size()) {
+                for (uint64_t j = Grp::rank(); j < q; j += Grp::size()) {
                     uint64_t i = ins0(j, fa) | (pass ? fb : 0ull);
                     uint64_t a0 = pass ? ((i & ~fb) | half) : i;
                     uint64_t a1 = a0 | fb;
-                    T x = v[a0], y = v[a1];
-                    v[i] = cscale(bx ? csub(x, y) : cadd(x, y), s);
+                    T x = A(a0), y = A(a1);
+                    A(i) = cscale(bx ? csub(x, y) : cadd(x, y), s);
                 }
-                G::sync();
+                Grp::sync();
             }
         }
         double pb = bx ? pm : pp;
@@ -801,26 +813,26 @@ struct Shot {
 
     // ------------------------------------------------- classical / noise
     // apply_pauli_to_frame (svm_kernels.inl:1812-1865)
-    __device__ void apply_pauli(const uint64_t* ex, const uint64_t* ez, int sign) {
+    __device__ __forceinline__ void apply_pauli(const uint64_t* ex, const uint64_t* ez, int sign) {
         int par = 0;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) par += __popcll(f.x[w] & ez[w]);
+        for (int w = 0; w < NW; ++w) par += __popcll(f.x[w] & __ldg(ez + w));
         if (par & 1) negate_gamma();
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
-            f.x[w] ^= ex[w];
-            f.z[w] ^= ez[w];
+            f.x[w] ^= __ldg(ex + w);
+            f.z[w] ^= __ldg(ez + w);
         }
         if (sign) negate_gamma();
     }
     // SchrodingerState::draw_next_noise (src/clifft/svm/svm.h:231-248)
-    __device__ void draw_next_noise() {
+    __device__ __forceinline__ void draw_next_noise() {
         const uint32_t n = P.n_sites;
         if (n == 0 || next_noise >= n) {
             next_noise = 0xffffffffu;
             return;
         }
-        double cur = next_noise == 0 ? 0.0 : P.hazards[next_noise - 1];
+        double cur = next_noise == 0 ? 0.0 : __ldg(P.hazards + next_noise - 1);
         double gap = -log(1.0 - uniform());
         double target = cur + gap;
         uint32_t lo = next_noise, hi = n;  // hazards are cumulative: answer >= next_noise
@@ -834,18 +846,18 @@ struct Shot {
         next_noise = lo;
     }
     // exec_noise (svm_kernels.inl:1886-1921)
-    __device__ void noise(uint32_t site) {
+    __device__ __forceinline__ void noise(uint32_t site) {
         if (site != next_noise) return;
-        const uint32_t c0 = P.site_off[site], c1 = P.site_off[site + 1];
+        const uint32_t c0 = __ldg(P.site_off + site), c1 = __ldg(P.site_off + site + 1);
         if (K.flags & KF_FORCED_FAULTS) {
             uint32_t c = c0 + K.fault_chan[ff_pos - 1];
             if (c < c1) apply_pauli(P.chan_x + (size_t)c * NW, P.chan_z + (size_t)c * NW, 0);
             next_noise = ff_pos < ff_end ? K.fault_sites[ff_pos++] : 0xffffffffu;
             return;
         }
-        double r = uniform() * P.site_psum[site], cum = 0.0;
+        double r = uniform() * __ldg(P.site_psum + site), cum = 0.0;
         for (uint32_t c = c0; c < c1; ++c) {
-            cum += P.chan_prob[c];
+            cum += __ldg(P.chan_prob + c);
             if (r < cum) {
                 apply_pauli(P.chan_x + (size_t)c * NW, P.chan_z + (size_t)c * NW, 0);
                 break;
@@ -855,7 +867,7 @@ struct Shot {
         draw_next_noise();
     }
     // exec_readout_noise (svm_kernels.inl:1937-1959)
-    __device__ void readout_noise(uint32_t e) {
+    __device__ __forceinline__ void readout_noise(uint32_t e) {
         bool fire = false;
         if (K.flags & KF_FORCED_FAULTS) {
             if (ro_pos < ro_end && K.ro_entries[ro_pos] == e) {
@@ -863,22 +875,23 @@ struct Shot {
                 ro_pos++;
             }
         } else {
-            fire = uniform() < P.ro_prob[e];
+            fire = uniform() < __ldg(P.ro_prob + e);
         }
         if (fire) {
             flush_records();
-            uint32_t mi = P.ro_meas[e];
-            if (G::rank() == 0) sh.rec[mi >> 5] ^= 1u << (mi & 31);
+            uint32_t mi = __ldg(P.ro_meas + e);
+            if (Grp::rank() == 0) rec[(mi >> 5) * S] ^= 1u << (mi & 31);
             rec_dirty = true;
         }
     }
     __device__ __forceinline__ int list_parity(const uint32_t* off, const uint32_t* tg, uint32_t l) {
         int p = 0;
-        for (uint32_t i = off[l]; i < off[l + 1]; ++i) p ^= rec_get(sh.rec, tg[i]);
+        const uint32_t e = __ldg(off + l + 1);
+        for (uint32_t i = __ldg(off + l); i < e; ++i) p ^= bit_of(rec, __ldg(tg + i), S);
         return p;
     }
     // exec_exp_val (svm_kernels.inl:2031-2173)
-    __device__ void exp_val(uint32_t cp, uint32_t out_idx) {
+    __device__ __forceinline__ void exp_val(uint32_t cp, uint32_t out_idx) {
         const uint64_t* mx = P.exp_x + (size_t)cp * NW;
         const uint64_t* mz = P.exp_z + (size_t)cp * NW;
         int fsign = P.exp_sign[cp] != 0;
@@ -906,8 +919,8 @@ struct Shot {
             if (fsign) iph = make_double2(-iph.x, -iph.y);
             double acc[3] = {0.0, 0.0, 0.0};
             const uint64_t dim = 1ull << k;
-            for (uint64_t j = G::rank(); j < dim; j += G::size()) {
-                T a = v[j], b = v[j ^ xa];
+            for (uint64_t j = Grp::rank(); j < dim; j += Grp::size()) {
+                T a = A(j), b = A(j ^ xa);
                 double ar = (double)a.x, ai = (double)a.y, br = (double)b.x, bi = -(double)b.y;
                 acc[2] += ar * ar + ai * ai;
                 double zs = (__popcll(j & za) & 1) ? -1.0 : 1.0;
@@ -916,17 +929,17 @@ struct Shot {
                 acc[0] += br * ar - bi * ai;
                 acc[1] += br * ai + bi * ar;
             }
-            group_reduce<G, 3>(acc, sh.red);
+            group_reduce<Grp, 3>(acc, red);
             account(1ull << k);
             double2 num = dmul(make_double2(acc[0], acc[1]), iph);
             if (acc[2] > 0.0) result = num.x / acc[2];
             result = fmin(1.0, fmax(-1.0, result));
         }
-        if (G::rank() == 0 && K.out_exp) K.out_exp[shot * P.num_exp + out_idx] = result;
+        if (Grp::rank() == 0 && K.out_exp) K.out_exp[shot * P.num_exp + out_idx] = result;
     }
 
     // ------------------------------------------------------------ driver
-    __device__ void run() {
+    __device__ __forceinline__ void run(Tally& tally) {
         // SchrodingerState::reset (svm_state.cc:220-267): only v[0] needs a
         // value; every other amplitude is written by EXPAND before it is read.
         f.clear();
@@ -942,12 +955,13 @@ struct Shot {
         rec_dirty = false;
         forced = (K.flags & KF_FORCED_MEAS) ? K.forced_meas + shot * P.slots : nullptr;
         meas_prob = (K.flags & KF_TRACE) && K.out_meas_prob ? K.out_meas_prob + shot * P.slots : nullptr;
-        for (uint32_t i = G::rank(); i < K.rec_words; i += G::size()) sh.rec[i] = 0;
-        for (uint32_t i = G::rank(); i < K.det_words; i += G::size()) sh.det[i] = 0;
-        for (uint32_t i = G::rank(); i < K.obs_words; i += G::size()) sh.obs[i] = 0;
+        for (uint32_t i = Grp::rank(); i < K.rec_words; i += Grp::size()) rec[i * S] = 0;
+        for (uint32_t i = Grp::rank(); i < K.det_words; i += Grp::size()) det[i * S] = 0;
+        for (uint32_t i = Grp::rank(); i < K.obs_words; i += Grp::size()) obs[i * S] = 0;
         if (meas_prob)
-            for (uint32_t i = G::rank(); i < P.slots; i += G::size()) meas_prob[i] = __longlong_as_double(0x7ff8000000000000ll);
-        if (G::rank() == 0) v[0] = Cx<R>::make(1.0, 0.0);
+            for (uint32_t i = Grp::rank(); i < P.slots; i += Grp::size())
+                meas_prob[i] = __longlong_as_double(0x7ff8000000000000ll);
+        if (Grp::rank() == 0) A(0) = Cx<R>::make(1.0, 0.0);
         if (K.flags & KF_FORCED_FAULTS) {
             ff_pos = K.fault_off[shot];
             ff_end = K.fault_off[shot + 1];
@@ -961,11 +975,12 @@ struct Shot {
             next_noise = 0;
             draw_next_noise();
         }
-        G::sync();
+        Grp::sync();
 
         const uint4* ip = P.instr;
-        for (uint32_t pc = 0; pc < P.n_instr && !stop; ++pc) {
-            const uint4 w0 = __ldg(ip + 2 * pc), w1 = __ldg(ip + 2 * pc + 1);
+        const uint32_t n_instr = P.n_instr;
+        for (uint32_t pc = 0; pc < n_instr; ++pc) {
+            const uint4 w0 = __ldg(ip + 2 * pc);
             uint32_t op = w0.x & 0xffu;
             const uint32_t fl = (w0.x >> 16) & 0xffu;
             const uint32_t a1 = w0.y & 0xffffu, a2 = w0.y >> 16;
@@ -987,28 +1002,32 @@ struct Shot {
                 case CLIFFT_OP_ARRAY_MULTI_CZ: array_multi_cz(a1, ((uint64_t)p1 << 32) | p0); break;
                 case CLIFFT_OP_ARRAY_H: array_h(a1); break;
                 case CLIFFT_OP_ARRAY_S:
-                    if (k > a1) phase_sweep(a1, 0.0, 1.0);
+                    phase_sweep(a1, 0.0, 1.0);
                     frame_s(a1, false);
                     break;
                 case CLIFFT_OP_ARRAY_S_DAG:
-                    if (k > a1) phase_sweep(a1, 0.0, -1.0);
+                    phase_sweep(a1, 0.0, -1.0);
                     frame_s(a1, true);
                     break;
                 case CLIFFT_OP_ARRAY_T: array_rot(a1, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
                 case CLIFFT_OP_ARRAY_T_DAG: array_rot(a1, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_ARRAY_ROT:
+                case CLIFFT_OP_ARRAY_ROT: {
+                    const uint4 w1 = __ldg(ip + 2 * pc + 1);
                     array_rot(a1, __longlong_as_double(((long long)p1 << 32) | p0),
                               __longlong_as_double(((long long)w1.y << 32) | w1.x));
                     break;
+                }
                 case CLIFFT_OP_ARRAY_U2: array_u2(a1, p0); break;
                 case CLIFFT_OP_ARRAY_U4: array_u4(a1, a2, p0); break;
                 case CLIFFT_OP_EXPAND: expand(a1, false, 0.0, 0.0); break;
                 case CLIFFT_OP_EXPAND_T: expand(a1, true, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
                 case CLIFFT_OP_EXPAND_T_DAG: expand(a1, true, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_EXPAND_ROT:
+                case CLIFFT_OP_EXPAND_ROT: {
+                    const uint4 w1 = __ldg(ip + 2 * pc + 1);
                     expand(a1, true, __longlong_as_double(((long long)p1 << 32) | p0),
                            __longlong_as_double(((long long)w1.y << 32) | w1.x));
                     break;
+                }
                 case CLIFFT_OP_MEAS_DORMANT_STATIC:
                     meas_dormant_static(a1, p0, sign, (fl & CLIFFT_FLAG_IDENTITY) != 0);
                     break;
@@ -1018,7 +1037,7 @@ struct Shot {
                 case CLIFFT_OP_SWAP_MEAS_INTERFERE: meas_interfere(a1, a2, p0, sign); break;
                 case CLIFFT_OP_APPLY_PAULI:
                     flush_records();
-                    if (rec_get(sh.rec, p1))
+                    if (bit_of(rec, p1, S))
                         apply_pauli(P.pauli_x + (size_t)p0 * NW, P.pauli_z + (size_t)p0 * NW,
                                     P.pauli_sign[p0] != 0);
                     break;
@@ -1031,7 +1050,7 @@ struct Shot {
                     flush_records();
                     int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
                     par ^= list_parity(P.det_off, P.det_tg, p0);
-                    if (G::rank() == 0 && par) sh.det[p1 >> 5] |= 1u << (p1 & 31);
+                    if (Grp::rank() == 0 && par) det[(p1 >> 5) * S] |= 1u << (p1 & 31);
                     break;
                 }
                 case CLIFFT_OP_POSTSELECT: {
@@ -1047,31 +1066,33 @@ struct Shot {
                 case CLIFFT_OP_OBSERVABLE: {
                     flush_records();
                     int par = list_parity(P.obs_off, P.obs_tg, p0);
-                    if (G::rank() == 0 && par) sh.obs[p1 >> 5] ^= 1u << (p1 & 31);
+                    if (Grp::rank() == 0 && par) obs[(p1 >> 5) * S] ^= 1u << (p1 & 31);
                     break;
                 }
                 case CLIFFT_OP_EXP_VAL: exp_val(p0, p1); break;
                 default:
-                    if (G::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_BAD_OPCODE);
+                    if (Grp::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_BAD_OPCODE);
                     stop = true;
                     break;
             }
+            if (stop) break;
         }
-        G::sync();
-        finish();
+        Grp::sync();
+        finish(tally);
     }
 
-    __device__ void finish() {
+    __device__ __forceinline__ void finish(Tally& tally) {
         const bool survived = !discarded && reachable;
-        const int r = G::rank();
+        const int r = Grp::rank();
         // observables XOR expected_observables (svm.cc:236-245)
         if (r == 0)
             for (uint32_t i = 0; i < P.num_obs && i < P.n_expected; ++i)
-                if (P.expected[i]) sh.obs[i >> 5] ^= 1u << (i & 31);
-        G::sync();
+                if (P.expected[i]) obs[(i >> 5) * S] ^= 1u << (i & 31);
+        Grp::sync();
         if (K.out_meas)
-            for (uint32_t w = r; w < K.meas_out_words; w += G::size()) {
-                uint64_t lo = sh.rec[2 * w], hi = (2 * w + 1 < K.rec_words) ? sh.rec[2 * w + 1] : 0u;
+            for (uint32_t w = r; w < K.meas_out_words; w += Grp::size()) {
+                uint64_t lo = rec[2 * w * S];
+                uint64_t hi = (2 * w + 1 < K.rec_words) ? rec[(2 * w + 1) * S] : 0u;
                 uint64_t word = lo | (hi << 32);
                 uint32_t base = w * 64;
                 if (base + 64 > P.num_meas) {
@@ -1081,13 +1102,15 @@ struct Shot {
                 K.out_meas[shot * K.meas_out_words + w] = word;
             }
         if (K.out_det)
-            for (uint32_t w = r; w < K.det_out_words; w += G::size()) {
-                uint64_t lo = sh.det[2 * w], hi = (2 * w + 1 < K.det_words) ? sh.det[2 * w + 1] : 0u;
+            for (uint32_t w = r; w < K.det_out_words; w += Grp::size()) {
+                uint64_t lo = det[2 * w * S];
+                uint64_t hi = (2 * w + 1 < K.det_words) ? det[(2 * w + 1) * S] : 0u;
                 K.out_det[shot * K.det_out_words + w] = lo | (hi << 32);
             }
         if (K.out_obs)
-            for (uint32_t w = r; w < K.obs_out_words; w += G::size()) {
-                uint64_t lo = sh.obs[2 * w], hi = (2 * w + 1 < K.obs_words) ? sh.obs[2 * w + 1] : 0u;
+            for (uint32_t w = r; w < K.obs_out_words; w += Grp::size()) {
+                uint64_t lo = obs[2 * w * S];
+                uint64_t hi = (2 * w + 1 < K.obs_words) ? obs[(2 * w + 1) * S] : 0u;
                 K.out_obs[shot * K.obs_out_words + w] = lo | (hi << 32);
             }
         if (r == 0) {
@@ -1104,68 +1127,97 @@ struct Shot {
                 if (K.out_final_pz) K.out_final_pz[shot * NW + w] = f.z[w];
             }
             if (survived && (K.flags & KF_SURVIVORS)) {
-                atomicAdd(K.counters + 0, 1ull);
+                tally.passed++;
                 bool any = false;
                 for (uint32_t i = 0; i < P.num_obs; ++i)
-                    if ((sh.obs[i >> 5] >> (i & 31)) & 1u) {
+                    if ((obs[(i >> 5) * S] >> (i & 31)) & 1u) {
                         any = true;
                         atomicAdd(K.counters + 4 + i, 1ull);
                     }
-                if (any) atomicAdd(K.counters + 1, 1ull);
+                if (any) tally.logical++;
             }
-            if (dust) atomicAdd(K.counters + 2, dust);
-            if (bytes) atomicAdd(K.counters + 3, bytes);
+            tally.dust += dust;
+            tally.bytes += bytes;
         }
         if (K.out_final_v && shot < K.dump_shots) {
             const uint64_t stride = 1ull << P.peak, n = 1ull << k;
             double* row = K.out_final_v + shot * stride * 2;
-            for (uint64_t i = r; i < stride; i += G::size()) {
+            for (uint64_t i = r; i < stride; i += Grp::size()) {
                 double re = 0.0, im = 0.0;
                 if (i < n) {
-                    re = (double)v[i].x;
-                    im = (double)v[i].y;
+                    re = (double)A(i).x;
+                    im = (double)A(i).y;
                 }
                 row[2 * i] = re;
                 row[2 * i + 1] = im;
             }
         }
-        G::sync();
+        Grp::sync();
     }
 };
 
 // ------------------------------------------------------------------ kernel
-template <typename R, class G, int NW>
-__global__ void __launch_bounds__(1024) svm_sample_kernel(const DevProg P, const KParams K) {
+// Shared memory per warp (G > 0) or per CTA (G = 0):
+//   [interleaved statevectors: 2^peak x S amplitudes, when state_in_smem]
+//   [records: (rec_words + det_words + obs_words) x S u32, interleaved]
+// then, for the whole block: 3 doubles per warp of reduction scratch and a
+// broadcast slot.
+template <int G>
+__host__ __device__ constexpr int shots_per_group_region() {
+    return G == 0 ? 1 : 32 / G;
+}
+
+template <typename R, int G, int NW>
+__global__ void __launch_bounds__(G == 0 ? 512 : 256) svm_sample_kernel(const DevProg P, const KParams K) {
+    using Grp = typename GroupOf<G>::type;
     using T = typename Cx<R>::T;
+    constexpr int S = Grp::S;
     extern __shared__ __align__(16) unsigned char smem[];
-    const int gl = G::local();
-    const int per_block = G::per_block();
-    // shared layout per group: [state (optional)] [rec] [det] [obs]; then
-    // block-wide: reduction scratch (3 doubles per warp) + broadcast slot.
-    const size_t state_bytes = K.state_in_smem ? (size_t)K.state_stride * sizeof(T) : 0;
-    const size_t rec_bytes = (size_t)(K.rec_words + K.det_words + K.obs_words) * 4;
-    const size_t group_bytes = (state_bytes + rec_bytes + 15) & ~(size_t)15;
-    unsigned char* gbase = smem + (size_t)gl * group_bytes;
-    unsigned char* tail = smem + (size_t)per_block * group_bytes;
-    GroupShared sh;
-    sh.rec = reinterpret_cast<uint32_t*>(gbase + state_bytes);
-    sh.det = sh.rec + K.rec_words;
-    sh.obs = sh.det + K.det_words;
-    sh.red = reinterpret_cast<double*>(tail);
-    sh.bcast = reinterpret_cast<unsigned long long*>(tail + 3 * sizeof(double) * (blockDim.x >> 5));
+    const int region = Grp::kCta ? 0 : (int)(threadIdx.x >> 5);
+    const int regions = Grp::kCta ? 1 : (int)(blockDim.x >> 5);
+    const size_t state_bytes = K.state_in_smem ? (size_t)K.state_stride * S * sizeof(T) : 0;
+    const size_t rec_bytes = (size_t)(K.rec_words + K.det_words + K.obs_words) * S * 4;
+    const size_t region_bytes = (state_bytes + rec_bytes + 15) & ~(size_t)15;
+    unsigned char* rbase = smem + (size_t)region * region_bytes;
+    unsigned char* tail = smem + (size_t)regions * region_bytes;
+    double* red = reinterpret_cast<double*>(tail);
+    unsigned long long* bcast =
+        reinterpret_cast<unsigned long long*>(tail + 3 * sizeof(double) * (blockDim.x >> 5));
+    uint32_t* rec = reinterpret_cast<uint32_t*>(rbase + state_bytes) + Grp::slot();
+    uint32_t* det = rec + (size_t)K.rec_words * S;
+    uint32_t* obs = det + (size_t)K.det_words * S;
     T* v;
     if (K.state_in_smem) {
-        v = reinterpret_cast<T*>(gbase);
+        v = reinterpret_cast<T*>(rbase) + Grp::slot();
     } else {
-        const size_t gid = (size_t)blockIdx.x * per_block + gl;
-        v = reinterpret_cast<T*>(K.state_global) + gid * K.state_stride;
+        const size_t gid = (size_t)blockIdx.x * regions + region;
+        v = reinterpret_cast<T*>(K.state_global) + gid * K.state_stride * S + Grp::slot();
     }
+    Tally tally;
     for (;;) {
-        unsigned long long shot = group_next_shot<G>(K.work_counter, sh.bcast);
-        if (shot >= K.shots) break;
-        Shot<R, G, NW> s(P, K, v, sh, shot);
-        s.run();
+        unsigned long long base = 0;
+        if (Grp::kCta) {
+            if (threadIdx.x == 0) *bcast = atomicAdd(K.work_counter, 1ull);
+            __syncthreads();
+            base = *bcast;
+            __syncthreads();
+        } else {
+            if ((threadIdx.x & 31) == 0) base = atomicAdd(K.work_counter, (unsigned long long)S);
+            base = __shfl_sync(0xffffffffu, base, 0);
+        }
+        if (base >= K.shots) break;
+        const unsigned long long shot = base + Grp::slot();
+        if (shot < K.shots) {
+            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, shot);
+            s.run(tally);
+        }
+        if (!Grp::kCta) __syncwarp();
     }
+    // flush per-lane totals (only group leaders hold non-zero values)
+    if (tally.passed) atomicAdd(K.counters + 0, tally.passed);
+    if (tally.logical) atomicAdd(K.counters + 1, tally.logical);
+    if (tally.dust) atomicAdd(K.counters + 2, tally.dust);
+    if (tally.bytes) atomicAdd(K.counters + 3, tally.bytes);
 }
 
 }  // namespace cgpu

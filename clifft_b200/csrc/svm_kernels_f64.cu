@@ -1,0 +1,7 @@
+// Instantiates the FP64-statevector interpreter kernels (one per shot-group
+// width G and frame width NW); see svm_kernel.cuh.
+#include "svm_instantiate.cuh"
+
+namespace cgpu {
+KernelFn kernel_f64(int G, int nw) { return pick_kernel_impl<double>(G, nw); }
+}  // namespace cgpu

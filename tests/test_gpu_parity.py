@@ -110,13 +110,23 @@ def test_free_sampling_fp32_matches_oracle_streams(seed):
     assert mismatched < 0.01
 
 
-@pytest.mark.parametrize("group", [32, 64, 128, 256, 1024])
+@pytest.mark.parametrize("group", [1, 2, 4, 8, 16, 32, 64, 128, 256, 512])
 def test_launch_shape_independence(group):
     prog, d = load_case(os.path.join(os.path.dirname(__file__), "golden", "fuzz_k9.npz"))
     base = cb.run(prog, 300, 5, precision="fp64", group_threads=0)
     g = cb.run(prog, 300, 5, precision="fp64", group_threads=group)
+    assert g["group_threads"] == group
     assert np.array_equal(base["meas_words"], g["meas_words"])
     np.testing.assert_allclose(base["exp_vals"], g["exp_vals"], atol=1e-12)
+    # forced replay is shape independent to rounding
+    o = O.run(prog, 40, seed=9, rng=O.RNG_PHILOX)
+    fm = np.zeros((40, prog.total_meas_slots), np.uint8)
+    fm[:, :prog.num_measurements] = o["meas"]
+    f = forced_gpu(prog, fm, None, None, "fp64", group)
+    ref = O.run(prog, 40, forced_meas=fm, want_state=True)
+    np.testing.assert_allclose(np.nan_to_num(f["meas_prob"]), np.nan_to_num(ref["meas_prob"]), atol=1e-10)
+    np.testing.assert_allclose(amplitudes(f["final_gamma"], f["final_v"]),
+                               amplitudes(ref["final_gamma"], ref["final_v"]), atol=1e-10)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
