@@ -519,8 +519,9 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const uint64_t shots = args->shots;
         if (args->precision != CLIFFT_GPU_FP32 && args->precision != CLIFFT_GPU_FP64)
             invalid("precision must be CLIFFT_GPU_FP32 or CLIFFT_GPU_FP64");
-        if (args->group_threads != 0 && (args->group_threads % 32 != 0 || args->group_threads > 1024))
-            invalid("group_threads must be 0 or a multiple of 32 up to 1024");
+        const uint32_t gt = args->group_threads;
+        if (gt != 0 && !(gt <= 32 && (gt & (gt - 1)) == 0) && (gt % 32 != 0 || gt > 1024))
+            invalid("group_threads must be 0, a power of two up to 32, or a multiple of 32 up to 1024");
         const bool dev_ptrs = (args->flags & CLIFFT_GPU_DEVICE_PTRS) != 0;
         const bool forced_meas = (args->flags & CLIFFT_GPU_FORCED_MEAS) != 0;
         const bool forced_faults = (args->flags & CLIFFT_GPU_FORCED_FAULTS) != 0;

@@ -455,15 +455,43 @@ struct Shot {
     }
 
     // ---------------------------------------------------------- array ops
+    // Sweeps run in two phases per batch of U items (all loads, then all
+    // stores) so each thread keeps U independent memory requests in flight;
+    // U = 4 for CTA groups streaming large statevectors, 1 for the
+    // shared-memory resident sub-warp groups.
+    static constexpr int U = Grp::kCta ? 4 : 1;
+
+    template <class V, int UU = U, class Ld, class St>
+    __device__ __forceinline__ void sweep(uint64_t n, Ld ld, St st) {
+        const uint64_t step = (uint64_t)Grp::size();
+        for (uint64_t i0 = Grp::rank(); i0 < n; i0 += step * UU) {
+            V val[UU];
+#pragma unroll
+            for (int u = 0; u < UU; ++u)
+                if (i0 + u * step < n) val[u] = ld(i0 + u * step);
+#pragma unroll
+            for (int u = 0; u < UU; ++u)
+                if (i0 + u * step < n) st(val[u]);
+        }
+    }
+    struct P2 {
+        uint64_t i;
+        T x, y;
+    };
+    struct P1 {
+        uint64_t i;
+        T x;
+    };
+    struct P4 {
+        uint64_t i;
+        T x0, x1, x2, x3;
+    };
+
     // exec_array_cnot (svm_kernels.inl:124-252)
     __device__ __forceinline__ void array_cnot(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), cb = 1ull << c, tb = 1ull << t;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t b0 = ins00(i, c, t) | cb;
-            T a = A(b0), b = A(b0 | tb);
-            A(b0) = b;
-            A(b0 | tb) = a;
-        }
+        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, c, t) | cb; p.x = A(p.i); p.y = A(p.i | tb); return p; },
+                  [&](const P2& p) { A(p.i) = p.y; A(p.i | tb) = p.x; });
         Grp::sync();
         account(1ull << k);
         frame_cnot(c, t);
@@ -471,10 +499,8 @@ struct Shot {
     // exec_array_cz (svm_kernels.inl:255-365)
     __device__ __forceinline__ void array_cz(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), both = (1ull << c) | (1ull << t);
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t idx = ins00(i, c, t) | both;
-            A(idx) = cneg(A(idx));
-        }
+        sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins00(i, c, t) | both; p.x = A(p.i); return p; },
+                  [&](const P1& p) { A(p.i) = cneg(p.x); });
         Grp::sync();
         account(1ull << (k - 1));
         frame_cz(c, t);
@@ -482,12 +508,8 @@ struct Shot {
     // exec_array_swap (svm_kernels.inl:369-458)
     __device__ __forceinline__ void array_swap(uint32_t a, uint32_t b) {
         const uint64_t n = 1ull << (k - 2), ab = 1ull << a, bb = 1ull << b;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t base = ins00(i, a, b);
-            T x = A(base | ab), y = A(base | bb);
-            A(base | ab) = y;
-            A(base | bb) = x;
-        }
+        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, a, b); p.x = A(p.i | ab); p.y = A(p.i | bb); return p; },
+                  [&](const P2& p) { A(p.i | ab) = p.y; A(p.i | bb) = p.x; });
         Grp::sync();
         account(1ull << k);
         frame_swap(a, b);
@@ -495,14 +517,24 @@ struct Shot {
     // exec_array_multi_cnot (svm_kernels.inl:464-550)
     __device__ __forceinline__ void array_multi_cnot(uint32_t t, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), tb = 1ull << t;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t a = ins0(i, t);
-            if (__popcll(a & mask) & 1) {
-                T x = A(a), y = A(a | tb);
-                A(a) = y;
-                A(a | tb) = x;
-            }
-        }
+        sweep<P2>(n,
+                  [&](uint64_t i) {
+                      P2 p;
+                      p.i = ins0(i, t);
+                      if (__popcll(p.i & mask) & 1) {
+                          p.x = A(p.i);
+                          p.y = A(p.i | tb);
+                      } else {
+                          p.i = ~0ull;
+                      }
+                      return p;
+                  },
+                  [&](const P2& p) {
+                      if (p.i != ~0ull) {
+                          A(p.i) = p.y;
+                          A(p.i | tb) = p.x;
+                      }
+                  });
         Grp::sync();
         account(1ull << k);
         for (uint32_t c = 0; c < k; ++c)
@@ -511,25 +543,44 @@ struct Shot {
     // exec_array_multi_cz (svm_kernels.inl:558-635)
     __device__ __forceinline__ void array_multi_cz(uint32_t c, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), cb = 1ull << c;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t a = ins0(i, c) | cb;
-            if (__popcll(a & mask) & 1) A(a) = cneg(A(a));
-        }
+        sweep<P1>(n,
+                  [&](uint64_t i) {
+                      P1 p;
+                      p.i = ins0(i, c) | cb;
+                      if (__popcll(p.i & mask) & 1)
+                          p.x = A(p.i);
+                      else
+                          p.i = ~0ull;
+                      return p;
+                  },
+                  [&](const P1& p) {
+                      if (p.i != ~0ull) A(p.i) = cneg(p.x);
+                  });
         Grp::sync();
         account(1ull << k);
         for (uint32_t t = 0; t < k; ++t)
             if ((mask >> t) & 1ull) frame_cz(c, t);
     }
-    // exec_array_h (svm_kernels.inl:639-744)
+    // 2x2 butterfly on axis a: ARRAY_H and ARRAY_U2 (svm_kernels.inl:639-744,1087-1297)
+    __device__ __forceinline__ void butterfly(uint32_t a, T m00, T m01, T m10, T m11) {
+        const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
+        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
+                  [&](const P2& p) {
+                      A(p.i) = cadd(cmul(m00, p.x), cmul(m01, p.y));
+                      A(p.i | ab) = cadd(cmul(m10, p.x), cmul(m11, p.y));
+                  });
+        Grp::sync();
+        account(2ull << k);
+    }
+    // exec_array_h (svm_kernels.inl:639-744): (a +- b) / sqrt(2)
     __device__ __forceinline__ void array_h(uint32_t a) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const R s = (R)CGPU_INV_SQRT2;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t i0 = ins0(i, a), i1 = i0 | ab;
-            T x = A(i0), y = A(i1);
-            A(i0) = cscale(cadd(x, y), s);
-            A(i1) = cscale(csub(x, y), s);
-        }
+        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
+                  [&](const P2& p) {
+                      A(p.i) = cscale(cadd(p.x, p.y), s);
+                      A(p.i | ab) = cscale(csub(p.x, p.y), s);
+                  });
         Grp::sync();
         account(2ull << k);
         frame_h(a);
@@ -538,10 +589,8 @@ struct Shot {
     __device__ __forceinline__ void phase_sweep(uint32_t a, double re, double im) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const T ph = Cx<R>::make(re, im);
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t idx = ins0(i, a) | ab;
-            A(idx) = cmul(A(idx), ph);
-        }
+        sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins0(i, a) | ab; p.x = A(p.i); return p; },
+                  [&](const P1& p) { A(p.i) = cmul(p.x, ph); });
         Grp::sync();
         account(1ull << k);
     }
@@ -564,11 +613,13 @@ struct Shot {
     __device__ __forceinline__ void expand(uint32_t a, bool with_phase, double zr, double zi) {
         const uint64_t half = 1ull << k;
         int x = with_phase ? f.px(a) : 0;
+        const T ph = Cx<R>::make(with_phase ? zr : 1.0, with_phase ? (x ? -zi : zi) : 0.0);
         if (!with_phase) {
-            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(half + i) = A(i);
+            sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i); return p; },
+                      [&](const P1& p) { A(half + p.i) = p.x; });
         } else {
-            const T ph = Cx<R>::make(zr, x ? -zi : zi);
-            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(half + i) = cmul(A(i), ph);
+            sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i); return p; },
+                      [&](const P1& p) { A(half + p.i) = cmul(p.x, ph); });
         }
         Grp::sync();
         account(2ull << k);
@@ -586,17 +637,8 @@ struct Shot {
         Frame<NW>::put(f.x, a, out & 1);
         Frame<NW>::put(f.z, a, (out >> 1) & 1);
         if (a >= k) return;
-        const T m00 = Cx<R>::make(m[0], m[1]), m01 = Cx<R>::make(m[2], m[3]);
-        const T m10 = Cx<R>::make(m[4], m[5]), m11 = Cx<R>::make(m[6], m[7]);
-        const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t i0 = ins0(i, a), i1 = i0 | ab;
-            T x = A(i0), y = A(i1);
-            A(i0) = cadd(cmul(m00, x), cmul(m01, y));
-            A(i1) = cadd(cmul(m10, x), cmul(m11, y));
-        }
-        Grp::sync();
-        account(2ull << k);
+        butterfly(a, Cx<R>::make(m[0], m[1]), Cx<R>::make(m[2], m[3]), Cx<R>::make(m[4], m[5]),
+                  Cx<R>::make(m[6], m[7]));
     }
     // exec_array_u4 (svm_kernels.inl:1310-1531)
     __device__ __forceinline__ void array_u4(uint32_t lo, uint32_t hi, uint32_t cp) {
@@ -610,24 +652,34 @@ struct Shot {
         Frame<NW>::put(f.x, hi, (out >> 2) & 1);
         Frame<NW>::put(f.z, hi, (out >> 3) & 1);
         const uint64_t n = 1ull << (k - 2), lb = 1ull << lo, hb = 1ull << hi;
-        for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) {
-            uint64_t b = ins00(i, lo, hi);
-            T x0 = A(b), x1 = A(b | lb), x2 = A(b | hb), x3 = A(b | lb | hb);
-            T y[4];
+        T m[16];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) {
-                const double* row = e + r * 8;
-                T acc = cmul(Cx<R>::make(row[0], row[1]), x0);
-                acc = cadd(acc, cmul(Cx<R>::make(row[2], row[3]), x1));
-                acc = cadd(acc, cmul(Cx<R>::make(row[4], row[5]), x2));
-                acc = cadd(acc, cmul(Cx<R>::make(row[6], row[7]), x3));
-                y[r] = acc;
-            }
-            A(b) = y[0];
-            A(b | lb) = y[1];
-            A(b | hb) = y[2];
-            A(b | lb | hb) = y[3];
-        }
+        for (int j = 0; j < 16; ++j) m[j] = Cx<R>::make(e[2 * j], e[2 * j + 1]);
+        sweep<P4, (U > 2 ? 2 : U)>(n,
+                  [&](uint64_t i) {
+                      P4 p;
+                      p.i = ins00(i, lo, hi);
+                      p.x0 = A(p.i);
+                      p.x1 = A(p.i | lb);
+                      p.x2 = A(p.i | hb);
+                      p.x3 = A(p.i | lb | hb);
+                      return p;
+                  },
+                  [&](const P4& p) {
+                      T y[4];
+#pragma unroll
+                      for (int r = 0; r < 4; ++r) {
+                          T acc = cmul(m[r * 4 + 0], p.x0);
+                          acc = cadd(acc, cmul(m[r * 4 + 1], p.x1));
+                          acc = cadd(acc, cmul(m[r * 4 + 2], p.x2));
+                          acc = cadd(acc, cmul(m[r * 4 + 3], p.x3));
+                          y[r] = acc;
+                      }
+                      A(p.i) = y[0];
+                      A(p.i | lb) = y[1];
+                      A(p.i | hb) = y[2];
+                      A(p.i | lb | hb) = y[3];
+                  });
         Grp::sync();
         account(2ull << k);
     }
@@ -706,9 +758,23 @@ struct Shot {
         const uint64_t half = 1ull << (k - 1);
         int pxv = f.px(a), pzv = f.pz(a);
         double acc[2] = {0.0, 0.0};
-        for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
-            acc[0] += cnorm_d(A(i));
-            acc[1] += cnorm_d(A(i + half));
+        {
+            const uint64_t step = (uint64_t)Grp::size();
+            for (uint64_t i0 = Grp::rank(); i0 < half; i0 += step * U) {
+                T x[U], y[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (i0 + u * step < half) {
+                        x[u] = A(i0 + u * step);
+                        y[u] = A(i0 + u * step + half);
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (i0 + u * step < half) {
+                        acc[0] += cnorm_d(x[u]);
+                        acc[1] += cnorm_d(y[u]);
+                    }
+            }
         }
         group_reduce<Grp, 2>(acc, red);
         account(1ull << k);
@@ -726,7 +792,8 @@ struct Shot {
         int m_abs = b ^ pxv;
         if (b == 1 && pzv) negate_gamma();
         if (b == 1) {
-            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) A(i) = A(i + half);
+            sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i + half); return p; },
+                      [&](const P1& p) { A(p.i) = p.x; });
             Grp::sync();
             account(1ull << k);
         }
@@ -749,18 +816,27 @@ struct Shot {
         int pxv = f.px(t), pzv = f.pz(t);
         const uint64_t half = 1ull << t, fb = 1ull << fa;
         double acc[2] = {0.0, 0.0};
-        for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
-            uint64_t a0, a1;
-            if (swapped) {
-                a0 = (i & ~fb) | (((i >> fa) & 1ull) << t);
-                a1 = a0 | fb;
-            } else {
-                a0 = i;
-                a1 = i + half;
+        {
+            const uint64_t step = (uint64_t)Grp::size();
+            for (uint64_t i0 = Grp::rank(); i0 < half; i0 += step * U) {
+                T x[U], y[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t i = i0 + u * step;
+                    if (i < half) {
+                        uint64_t a0 = swapped ? ((i & ~fb) | (((i >> fa) & 1ull) << t)) : i;
+                        uint64_t a1 = swapped ? (a0 | fb) : (i + half);
+                        x[u] = A(a0);
+                        y[u] = A(a1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (i0 + u * step < half) {
+                        acc[0] += cnorm_d(cadd(x[u], y[u]));
+                        acc[1] += cnorm_d(csub(x[u], y[u]));
+                    }
             }
-            T x = A(a0), y = A(a1);
-            acc[0] += cnorm_d(cadd(x, y));
-            acc[1] += cnorm_d(csub(x, y));
         }
         group_reduce<Grp, 2>(acc, red);
         account((1ull << k) * 2 + (1ull << (k - 1)));
@@ -778,21 +854,22 @@ struct Shot {
         int m_abs = bx ^ pzv;
         const R s = (R)CGPU_INV_SQRT2;
         if (!swapped) {
-            for (uint64_t i = Grp::rank(); i < half; i += Grp::size()) {
-                T x = A(i), y = A(i + half);
-                A(i) = cscale(bx ? csub(x, y) : cadd(x, y), s);
-            }
+            sweep<P2>(half, [&](uint64_t i) { P2 p; p.i = i; p.x = A(i); p.y = A(i + half); return p; },
+                      [&](const P2& p) { A(p.i) = cscale(bx ? csub(p.x, p.y) : cadd(p.x, p.y), s); });
             Grp::sync();
         } else {
             const uint64_t q = half >> 1;  // outputs with bit fa clear, then set
             for (int pass = 0; pass < 2; ++pass) {
-                for (uint64_t j = Grp::rank(); j < q; j += Grp::size()) {
-                    uint64_t i = ins0(j, fa) | (pass ? fb : 0ull);
-                    uint64_t a0 = pass ? ((i & ~fb) | half) : i;
-                    uint64_t a1 = a0 | fb;
-                    T x = A(a0), y = A(a1);
-                    A(i) = cscale(bx ? csub(x, y) : cadd(x, y), s);
-                }
+                sweep<P2>(q,
+                          [&](uint64_t j) {
+                              P2 p;
+                              p.i = ins0(j, fa) | (pass ? fb : 0ull);
+                              uint64_t a0 = pass ? ((p.i & ~fb) | half) : p.i;
+                              p.x = A(a0);
+                              p.y = A(a0 | fb);
+                              return p;
+                          },
+                          [&](const P2& p) { A(p.i) = cscale(bx ? csub(p.x, p.y) : cadd(p.x, p.y), s); });
                 Grp::sync();
             }
         }
@@ -919,15 +996,29 @@ struct Shot {
             if (fsign) iph = make_double2(-iph.x, -iph.y);
             double acc[3] = {0.0, 0.0, 0.0};
             const uint64_t dim = 1ull << k;
-            for (uint64_t j = Grp::rank(); j < dim; j += Grp::size()) {
-                T a = A(j), b = A(j ^ xa);
-                double ar = (double)a.x, ai = (double)a.y, br = (double)b.x, bi = -(double)b.y;
-                acc[2] += ar * ar + ai * ai;
-                double zs = (__popcll(j & za) & 1) ? -1.0 : 1.0;
-                ar *= zs;
-                ai *= zs;
-                acc[0] += br * ar - bi * ai;
-                acc[1] += br * ai + bi * ar;
+            const uint64_t step = (uint64_t)Grp::size();
+            for (uint64_t j0 = Grp::rank(); j0 < dim; j0 += step * U) {
+                T av[U], bv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (j0 + u * step < dim) {
+                        av[u] = A(j0 + u * step);
+                        bv[u] = A((j0 + u * step) ^ xa);
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t j = j0 + u * step;
+                    if (j < dim) {
+                        double ar = (double)av[u].x, ai = (double)av[u].y;
+                        double br = (double)bv[u].x, bi = -(double)bv[u].y;
+                        acc[2] += ar * ar + ai * ai;
+                        double zs = (__popcll(j & za) & 1) ? -1.0 : 1.0;
+                        ar *= zs;
+                        ai *= zs;
+                        acc[0] += br * ar - bi * ai;
+                        acc[1] += br * ai + bi * ar;
+                    }
+                }
             }
             group_reduce<Grp, 3>(acc, red);
             account(1ull << k);
@@ -1168,7 +1259,7 @@ __host__ __device__ constexpr int shots_per_group_region() {
 }
 
 template <typename R, int G, int NW>
-__global__ void __launch_bounds__(G == 0 ? 512 : 256) svm_sample_kernel(const DevProg P, const KParams K) {
+__global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const DevProg P, const KParams K) {
     using Grp = typename GroupOf<G>::type;
     using T = typename Cx<R>::T;
     constexpr int S = Grp::S;

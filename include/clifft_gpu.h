@@ -69,7 +69,7 @@ typedef struct clifft_gpu_sample_args {
     uint64_t first_shot;    /* global index of shot 0 (multi-GPU shards, resumption) */
     uint32_t precision;     /* CLIFFT_GPU_FP64 or CLIFFT_GPU_FP32 */
     uint32_t flags;
-    uint32_t group_threads; /* 0 = autotuned; 32 = one warp per shot; 64..1024 = one CTA per shot */
+    uint32_t group_threads; /* 0 = automatic; 1,2,4..32 = lanes per shot (32/G shots per warp); 64..1024 = one CTA per shot */
     uint32_t reserved;
     double dust_eps;        /* relative dust threshold; 0 = 1e-18 (FP64) / 1e-9 (FP32) */
     /* CLIFFT_GPU_FORCED_MEAS: shots x total_meas_slots bytes (0/1) */
