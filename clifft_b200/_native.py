@@ -21,6 +21,7 @@ CLIFFT_GPU_FORCED_MEAS = 0x02
 CLIFFT_GPU_FORCED_FAULTS = 0x04
 CLIFFT_GPU_DEVICE_PTRS = 0x08
 CLIFFT_GPU_TRACE = 0x10
+CLIFFT_GPU_NO_FUSION = 0x20
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device error", -4: "out of memory"}
 
@@ -45,9 +46,10 @@ class Outputs(ctypes.Structure):
         ("final_px", P), ("final_pz", P), ("final_v", P), ("dump_shots", ctypes.c_uint64),
         ("passed_shots", ctypes.c_uint64), ("logical_errors", ctypes.c_uint64),
         ("observable_ones", P), ("dust_clamps", ctypes.c_uint64),
-        ("algorithmic_bytes", ctypes.c_uint64),
+        ("algorithmic_bytes", ctypes.c_uint64), ("streamed_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_float),
         ("group_threads", ctypes.c_uint32), ("state_in_smem", ctypes.c_uint32),
+        ("fused", ctypes.c_uint32),
     ]
 
 

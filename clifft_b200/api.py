@@ -86,7 +86,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         faults: Optional[Sequence[Sequence[tuple]]] = None,
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
-        dust_eps: float = 0.0, want_records: bool = True) -> Dict[str, object]:
+        dust_eps: float = 0.0, want_records: bool = True, fusion: bool = True) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports."""
     if precision not in _PRECISIONS:
@@ -121,6 +121,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_FORCED_FAULTS
     if trace:
         flags |= N.CLIFFT_GPU_TRACE
+    if not fusion:
+        flags |= N.CLIFFT_GPU_NO_FUSION
     a.flags = flags
     o = N.Outputs()
     if want_records:
@@ -156,7 +158,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         res["final_v"] = fv[..., 0] + 1j * fv[..., 1]
     res.update(passed_shots=int(o.passed_shots), logical_errors=int(o.logical_errors),
                observable_ones=ones[:p.num_observables].copy(), dust_clamps=int(o.dust_clamps),
-               algorithmic_bytes=int(o.algorithmic_bytes),
+               algorithmic_bytes=int(o.algorithmic_bytes), streamed_bytes=int(o.streamed_bytes),
+               fused=bool(o.fused),
                kernel_ms=float(o.kernel_ms), kernel_launches=int(o.kernel_launches),
                group_threads=int(o.group_threads), state_in_smem=bool(o.state_in_smem))
     return res
@@ -164,7 +167,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
 
 def _stats(r) -> dict:
     return {k: r[k] for k in ("kernel_ms", "kernel_launches", "group_threads", "state_in_smem",
-                              "dust_clamps", "algorithmic_bytes")}
+                              "dust_clamps", "algorithmic_bytes", "streamed_bytes", "fused")}
 
 
 def sample(program: Program, shots: int, seed: Optional[int] = None, *,

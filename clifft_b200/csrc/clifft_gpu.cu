@@ -279,6 +279,7 @@ struct LaunchPlan {
     bool state_in_smem;
     uint64_t state_stride;
     uint32_t nw_words;
+    bool fuse;
 };
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
@@ -294,7 +295,8 @@ int default_group(uint32_t peak) {
 }
 
 LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
-                       uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words) {
+                       uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words,
+                       bool allow_fusion) {
     LaunchPlan L{};
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const uint64_t stride = uint64_t(1) << p.meta.peak_rank;
@@ -324,7 +326,11 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
     const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
     auto region_bytes = [&](bool in_smem) {
-        return ((in_smem ? state_bytes * L.S : 0) + rec_bytes1 * L.S + 15) & ~size_t(15);
+        size_t fuse = 0;
+        if (G == 0 && !in_smem && allow_fusion)
+            fuse = precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>() : fuse_smem_bytes<double>();
+        return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
+               ~size_t(15);
     };
     auto tail = [&](int threads) { return size_t(3 * 8 * (threads / 32) + 64); };
     if (G) {
@@ -341,6 +347,7 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         L.regions = 1;
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
+    L.fuse = G == 0 && !L.state_in_smem && allow_fusion;
     L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
     CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -533,6 +540,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->logical_errors = 0;
         out->dust_clamps = 0;
         out->algorithmic_bytes = 0;
+        out->streamed_bytes = 0;
         out->kernel_launches = 0;
         out->kernel_ms = 0.f;
         if (shots == 0) return;
@@ -559,7 +567,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const uint32_t det_words = (m.num_detectors + 31) / 32;
         const uint32_t obs_words = (m.num_observables + 31) / 32;
         LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words,
-                                   det_words, obs_words);
+                                   det_words, obs_words, (args->flags & CLIFFT_GPU_NO_FUSION) == 0);
 
         KParams K{};
         K.shots = shots;
@@ -568,7 +576,10 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         K.dust_eps = args->dust_eps > 0.0 ? args->dust_eps : (args->precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
         K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
                   (forced_meas ? KF_FORCED_MEAS : 0) | (forced_faults ? KF_FORCED_FAULTS : 0) |
-                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0);
+                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0) | (L.fuse ? KF_FUSE : 0);
+        K.fuse_bytes = L.fuse ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
+                                                                   : fuse_smem_bytes<double>())
+                              : 0;
         K.rec_words = rec_words;
         K.det_words = det_words;
         K.obs_words = obs_words;
@@ -580,7 +591,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const size_t amp = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
         if (!L.state_in_smem)
             K.state_global = buf.alloc(size_t(L.blocks) * L.regions * L.S * L.state_stride * amp);
-        const size_t n_counters = 4 + m.num_observables;
+        const size_t n_counters = 5 + m.num_observables;
         auto* scratch = static_cast<unsigned long long*>(buf.alloc((2 + n_counters) * 8 + 64));
         CUDA_OK(cudaMemsetAsync(scratch, 0, (2 + n_counters) * 8 + 64, st));
         K.work_counter = scratch;
@@ -687,12 +698,14 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->logical_errors = hs[3];
         out->dust_clamps = hs[4];
         out->algorithmic_bytes = hs[5];
+        out->streamed_bytes = hs[6];
         if (out->observable_ones)
-            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[6 + i];
+            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[7 + i];
         out->kernel_launches = 1;
         out->kernel_ms = ms;
         out->group_threads = L.G ? uint32_t(L.G) : uint32_t(L.threads);
         out->state_in_smem = L.state_in_smem ? 1u : 0u;
+        out->fused = L.fuse ? 1u : 0u;
     });
 }
 

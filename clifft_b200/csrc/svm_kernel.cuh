@@ -97,7 +97,7 @@ struct KParams {
     uint64_t state_stride;    // amplitudes per shot slot (2^peak_rank)
     void* state_global;       // global slab base (when !state_in_smem)
     unsigned long long* work_counter;
-    unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3] algorithmic bytes, [4..] observable ones
+    unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3] algorithmic bytes, [4] streamed bytes, [5..] observable ones
     int* error_word;               // first device-side error code (0 = none)
     // forced inputs
     const uint8_t* forced_meas;
@@ -120,6 +120,7 @@ struct KParams {
     uint64_t* out_final_pz;
     double* out_final_v;
     uint64_t dump_shots;
+    uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
 };
 
 enum : uint32_t {
@@ -127,6 +128,7 @@ enum : uint32_t {
     KF_FORCED_MEAS = 0x02u,
     KF_FORCED_FAULTS = 0x04u,
     KF_TRACE = 0x10u,
+    KF_FUSE = 0x20u,  // fused tile sweeps for global-memory statevectors (CTA groups)
 };
 
 enum : int {
@@ -345,8 +347,45 @@ __device__ __forceinline__ int bit_of(const uint32_t* r, uint32_t i, int S) {
 
 // Per-lane totals flushed once per kernel.
 struct Tally {
-    unsigned long long passed = 0, logical = 0, dust = 0, bytes = 0;
+    unsigned long long passed = 0, logical = 0, dust = 0, bytes = 0, moved = 0;
 };
+
+// ------------------------------------------------------------- fused sweeps
+// A fused block is a run of consecutive array / frame opcodes whose active
+// axes fit in one tile of 2^TILE_BITS amplitudes. Its frame-dependent choices
+// (conjugated phases, U2 / U4 variants) are resolved once per shot into
+// micro-ops on tile-local bit positions; the statevector is then streamed tile
+// by tile through shared memory, applying every micro-op before writing back.
+// Each amplitude sees the same arithmetic in the same order as the unfused
+// opcode sequence.
+enum : uint8_t { M_CNOT, M_CZ, M_SWAP, M_MCNOT, M_MCZ, M_H, M_PHASE, M_U2, M_U4 };
+struct MicroOp {
+    uint8_t kind, a, b, pad;
+    uint32_t mask;  // local-bit mask (multi gates)
+    double c[32];   // up to 16 complex coefficients
+};
+constexpr int kMaxMicroOps = 24;
+template <typename R>
+struct TileCfg {
+    static constexpr int kBits = sizeof(R) == 4 ? 12 : 11;  // 32 KiB per tile buffer
+};
+template <typename R>
+__host__ __device__ constexpr uint32_t fuse_smem_bytes() {
+    return (uint32_t)(2u * (1u << TileCfg<R>::kBits) * 2u * sizeof(R) + kMaxMicroOps * sizeof(MicroOp) +
+                      2u * 64u * 8u + 64u);
+}
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // --------------------------------------------------------------- the shot
 template <typename R, class Grp, int NW>
@@ -376,13 +415,23 @@ struct Shot {
     unsigned long long bytes;  // algorithmic statevector bytes moved by this shot
     const uint8_t* forced;
     double* meas_prob;
+    // fused-sweep state (CTA groups only)
+    unsigned char* fuse;       // shared scratch: 2 tile buffers, micro-ops, index tables
+    bool resolving;            // true while a fused block's opcodes emit micro-ops
+    int n_mops;
+    unsigned long long moved;  // statevector bytes actually streamed
 
     __device__ __forceinline__ Shot(const DevProg& p, const KParams& kp, T* vv, uint32_t* r, uint32_t* d,
-                                    uint32_t* o, double* rd, uint64_t s)
-        : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s) {}
+                                    uint32_t* o, double* rd, unsigned char* fz, uint64_t s)
+        : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s), fuse(fz) {}
 
     __device__ __forceinline__ T& A(uint64_t i) { return v[i * S]; }
-    __device__ __forceinline__ void account(uint64_t amps) { bytes += amps * sizeof(T); }
+    // algorithmic bytes of an opcode (per-opcode definition); streamed bytes
+    // are counted separately because a fused block streams the state once
+    __device__ __forceinline__ void account(uint64_t amps) {
+        bytes += amps * sizeof(T);
+        if (!resolving) moved += amps * sizeof(T);
+    }
     __device__ __forceinline__ double uniform() { return philox_uniform(K.seed, K.first_shot + shot, draw++); }
     __device__ __forceinline__ void phase(double2 p) { gamma = dmul(gamma, p); }
     __device__ __forceinline__ void negate_gamma() { gamma = make_double2(-gamma.x, -gamma.y); }
@@ -487,55 +536,98 @@ struct Shot {
         T x0, x1, x2, x3;
     };
 
+    // micro-op emission while resolving a fused block (thread 0 writes; every
+    // thread computes the same values)
+    __device__ __forceinline__ uint8_t local_bit(uint32_t axis) const {
+        return reinterpret_cast<const uint8_t*>(fuse + fuse_lbit_offset())[axis];
+    }
+    static __host__ __device__ constexpr uint32_t fuse_mops_offset() {
+        return 2u * (1u << TileCfg<R>::kBits) * (uint32_t)sizeof(T);
+    }
+    static __host__ __device__ constexpr uint32_t fuse_tables_offset() {
+        return fuse_mops_offset() + kMaxMicroOps * (uint32_t)sizeof(MicroOp);
+    }
+    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return fuse_tables_offset() + 2u * 64u * 8u; }
+    __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
+                                         int nc) {
+        if (Grp::rank() == 0) {
+            MicroOp* m = reinterpret_cast<MicroOp*>(fuse + fuse_mops_offset()) + n_mops;
+            m->kind = kind;
+            m->a = local_bit(a);
+            m->b = local_bit(b);
+            uint32_t lm = 0;
+            for (uint64_t w = mask; w; w &= w - 1) lm |= 1u << local_bit((uint32_t)__ffsll((long long)w) - 1);
+            m->mask = lm;
+            for (int j = 0; j < nc; ++j) m->c[j] = c[j];
+        }
+        n_mops++;
+    }
+
     // exec_array_cnot (svm_kernels.inl:124-252)
     __device__ __forceinline__ void array_cnot(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), cb = 1ull << c, tb = 1ull << t;
-        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, c, t) | cb; p.x = A(p.i); p.y = A(p.i | tb); return p; },
-                  [&](const P2& p) { A(p.i) = p.y; A(p.i | tb) = p.x; });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_CNOT, c, t, 0, nullptr, 0);
+        } else {
+            sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, c, t) | cb; p.x = A(p.i); p.y = A(p.i | tb); return p; },
+                      [&](const P2& p) { A(p.i) = p.y; A(p.i | tb) = p.x; });
+            Grp::sync();
+        }
         account(1ull << k);
         frame_cnot(c, t);
     }
     // exec_array_cz (svm_kernels.inl:255-365)
     __device__ __forceinline__ void array_cz(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), both = (1ull << c) | (1ull << t);
-        sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins00(i, c, t) | both; p.x = A(p.i); return p; },
-                  [&](const P1& p) { A(p.i) = cneg(p.x); });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_CZ, c, t, 0, nullptr, 0);
+        } else {
+            sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins00(i, c, t) | both; p.x = A(p.i); return p; },
+                      [&](const P1& p) { A(p.i) = cneg(p.x); });
+            Grp::sync();
+        }
         account(1ull << (k - 1));
         frame_cz(c, t);
     }
     // exec_array_swap (svm_kernels.inl:369-458)
     __device__ __forceinline__ void array_swap(uint32_t a, uint32_t b) {
         const uint64_t n = 1ull << (k - 2), ab = 1ull << a, bb = 1ull << b;
-        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, a, b); p.x = A(p.i | ab); p.y = A(p.i | bb); return p; },
-                  [&](const P2& p) { A(p.i | ab) = p.y; A(p.i | bb) = p.x; });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_SWAP, a, b, 0, nullptr, 0);
+        } else {
+            sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, a, b); p.x = A(p.i | ab); p.y = A(p.i | bb); return p; },
+                      [&](const P2& p) { A(p.i | ab) = p.y; A(p.i | bb) = p.x; });
+            Grp::sync();
+        }
         account(1ull << k);
         frame_swap(a, b);
     }
     // exec_array_multi_cnot (svm_kernels.inl:464-550)
     __device__ __forceinline__ void array_multi_cnot(uint32_t t, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), tb = 1ull << t;
-        sweep<P2>(n,
-                  [&](uint64_t i) {
-                      P2 p;
-                      p.i = ins0(i, t);
-                      if (__popcll(p.i & mask) & 1) {
-                          p.x = A(p.i);
-                          p.y = A(p.i | tb);
-                      } else {
-                          p.i = ~0ull;
-                      }
-                      return p;
-                  },
-                  [&](const P2& p) {
-                      if (p.i != ~0ull) {
-                          A(p.i) = p.y;
-                          A(p.i | tb) = p.x;
-                      }
-                  });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_MCNOT, t, t, mask, nullptr, 0);
+        } else {
+            sweep<P2>(n,
+                      [&](uint64_t i) {
+                          P2 p;
+                          p.i = ins0(i, t);
+                          if (__popcll(p.i & mask) & 1) {
+                              p.x = A(p.i);
+                              p.y = A(p.i | tb);
+                          } else {
+                              p.i = ~0ull;
+                          }
+                          return p;
+                      },
+                      [&](const P2& p) {
+                          if (p.i != ~0ull) {
+                              A(p.i) = p.y;
+                              A(p.i | tb) = p.x;
+                          }
+                      });
+            Grp::sync();
+        }
         account(1ull << k);
         for (uint32_t c = 0; c < k; ++c)
             if ((mask >> c) & 1ull) frame_cnot(c, t);
@@ -543,55 +635,57 @@ struct Shot {
     // exec_array_multi_cz (svm_kernels.inl:558-635)
     __device__ __forceinline__ void array_multi_cz(uint32_t c, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), cb = 1ull << c;
-        sweep<P1>(n,
-                  [&](uint64_t i) {
-                      P1 p;
-                      p.i = ins0(i, c) | cb;
-                      if (__popcll(p.i & mask) & 1)
-                          p.x = A(p.i);
-                      else
-                          p.i = ~0ull;
-                      return p;
-                  },
-                  [&](const P1& p) {
-                      if (p.i != ~0ull) A(p.i) = cneg(p.x);
-                  });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_MCZ, c, c, mask, nullptr, 0);
+        } else {
+            sweep<P1>(n,
+                      [&](uint64_t i) {
+                          P1 p;
+                          p.i = ins0(i, c) | cb;
+                          if (__popcll(p.i & mask) & 1)
+                              p.x = A(p.i);
+                          else
+                              p.i = ~0ull;
+                          return p;
+                      },
+                      [&](const P1& p) {
+                          if (p.i != ~0ull) A(p.i) = cneg(p.x);
+                      });
+            Grp::sync();
+        }
         account(1ull << k);
         for (uint32_t t = 0; t < k; ++t)
             if ((mask >> t) & 1ull) frame_cz(c, t);
-    }
-    // 2x2 butterfly on axis a: ARRAY_H and ARRAY_U2 (svm_kernels.inl:639-744,1087-1297)
-    __device__ __forceinline__ void butterfly(uint32_t a, T m00, T m01, T m10, T m11) {
-        const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
-        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
-                  [&](const P2& p) {
-                      A(p.i) = cadd(cmul(m00, p.x), cmul(m01, p.y));
-                      A(p.i | ab) = cadd(cmul(m10, p.x), cmul(m11, p.y));
-                  });
-        Grp::sync();
-        account(2ull << k);
     }
     // exec_array_h (svm_kernels.inl:639-744): (a +- b) / sqrt(2)
     __device__ __forceinline__ void array_h(uint32_t a) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const R s = (R)CGPU_INV_SQRT2;
-        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
-                  [&](const P2& p) {
-                      A(p.i) = cscale(cadd(p.x, p.y), s);
-                      A(p.i | ab) = cscale(csub(p.x, p.y), s);
-                  });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            emit(M_H, a, a, 0, nullptr, 0);
+        } else {
+            sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
+                      [&](const P2& p) {
+                          A(p.i) = cscale(cadd(p.x, p.y), s);
+                          A(p.i | ab) = cscale(csub(p.x, p.y), s);
+                      });
+            Grp::sync();
+        }
         account(2ull << k);
         frame_h(a);
     }
     // apply_phase_waterfall (svm_kernels.inl:764-830)
     __device__ __forceinline__ void phase_sweep(uint32_t a, double re, double im) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
-        const T ph = Cx<R>::make(re, im);
-        sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins0(i, a) | ab; p.x = A(p.i); return p; },
-                  [&](const P1& p) { A(p.i) = cmul(p.x, ph); });
-        Grp::sync();
+        if (Grp::kCta && resolving) {
+            const double c[2] = {re, im};
+            emit(M_PHASE, a, a, 0, c, 2);
+        } else {
+            const T ph = Cx<R>::make(re, im);
+            sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins0(i, a) | ab; p.x = A(p.i); return p; },
+                      [&](const P1& p) { A(p.i) = cmul(p.x, ph); });
+            Grp::sync();
+        }
         account(1ull << k);
     }
     // exec_array_t / t_dag / rot (svm_kernels.inl:951-988,1044-1061)
@@ -637,8 +731,21 @@ struct Shot {
         Frame<NW>::put(f.x, a, out & 1);
         Frame<NW>::put(f.z, a, (out >> 1) & 1);
         if (a >= k) return;
-        butterfly(a, Cx<R>::make(m[0], m[1]), Cx<R>::make(m[2], m[3]), Cx<R>::make(m[4], m[5]),
-                  Cx<R>::make(m[6], m[7]));
+        if (Grp::kCta && resolving) {
+            emit(M_U2, a, a, 0, m, 8);
+            account(2ull << k);
+            return;
+        }
+        const T m00 = Cx<R>::make(m[0], m[1]), m01 = Cx<R>::make(m[2], m[3]);
+        const T m10 = Cx<R>::make(m[4], m[5]), m11 = Cx<R>::make(m[6], m[7]);
+        const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
+        sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
+                  [&](const P2& p) {
+                      A(p.i) = cadd(cmul(m00, p.x), cmul(m01, p.y));
+                      A(p.i | ab) = cadd(cmul(m10, p.x), cmul(m11, p.y));
+                  });
+        Grp::sync();
+        account(2ull << k);
     }
     // exec_array_u4 (svm_kernels.inl:1310-1531)
     __device__ __forceinline__ void array_u4(uint32_t lo, uint32_t hi, uint32_t cp) {
@@ -651,6 +758,11 @@ struct Shot {
         Frame<NW>::put(f.z, lo, (out >> 1) & 1);
         Frame<NW>::put(f.x, hi, (out >> 2) & 1);
         Frame<NW>::put(f.z, hi, (out >> 3) & 1);
+        if (Grp::kCta && resolving) {
+            emit(M_U4, lo, hi, 0, e, 32);
+            account(2ull << k);
+            return;
+        }
         const uint64_t n = 1ull << (k - 2), lb = 1ull << lo, hb = 1ull << hi;
         T m[16];
 #pragma unroll
@@ -1029,6 +1141,319 @@ struct Shot {
         if (Grp::rank() == 0 && K.out_exp) K.out_exp[shot * P.num_exp + out_idx] = result;
     }
 
+    // Executes instruction `pc` (the dispatch of execute_internal,
+    // svm_kernels.inl:2183-2646; forced opcodes share the sampling handlers).
+    __device__ __forceinline__ void exec(uint32_t pc) {
+        const uint4* ip = P.instr;
+        const uint4 w0 = __ldg(ip + 2 * pc);
+        uint32_t op = w0.x & 0xffu;
+        const uint32_t fl = (w0.x >> 16) & 0xffu;
+        const uint32_t a1 = w0.y & 0xffffu, a2 = w0.y >> 16;
+        const uint32_t p0 = w0.z, p1 = w0.w;
+        const int sign = (fl & CLIFFT_FLAG_SIGN) ? 1 : 0;
+        if (op >= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED)
+            op -= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED - CLIFFT_OP_MEAS_DORMANT_STATIC;
+            switch (op) {
+            case CLIFFT_OP_FRAME_CNOT: frame_cnot(a1, a2); break;
+            case CLIFFT_OP_FRAME_CZ: frame_cz(a1, a2); break;
+            case CLIFFT_OP_FRAME_H: frame_h(a1); break;
+            case CLIFFT_OP_FRAME_S: frame_s(a1, false); break;
+            case CLIFFT_OP_FRAME_S_DAG: frame_s(a1, true); break;
+            case CLIFFT_OP_FRAME_SWAP: frame_swap(a1, a2); break;
+            case CLIFFT_OP_ARRAY_CNOT: array_cnot(a1, a2); break;
+            case CLIFFT_OP_ARRAY_CZ: array_cz(a1, a2); break;
+            case CLIFFT_OP_ARRAY_SWAP: array_swap(a1, a2); break;
+            case CLIFFT_OP_ARRAY_MULTI_CNOT: array_multi_cnot(a1, ((uint64_t)p1 << 32) | p0); break;
+            case CLIFFT_OP_ARRAY_MULTI_CZ: array_multi_cz(a1, ((uint64_t)p1 << 32) | p0); break;
+            case CLIFFT_OP_ARRAY_H: array_h(a1); break;
+            case CLIFFT_OP_ARRAY_S:
+                phase_sweep(a1, 0.0, 1.0);
+                frame_s(a1, false);
+                break;
+            case CLIFFT_OP_ARRAY_S_DAG:
+                phase_sweep(a1, 0.0, -1.0);
+                frame_s(a1, true);
+                break;
+            case CLIFFT_OP_ARRAY_T: array_rot(a1, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
+            case CLIFFT_OP_ARRAY_T_DAG: array_rot(a1, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
+            case CLIFFT_OP_ARRAY_ROT: {
+                const uint4 w1 = __ldg(ip + 2 * pc + 1);
+                array_rot(a1, __longlong_as_double(((long long)p1 << 32) | p0),
+                          __longlong_as_double(((long long)w1.y << 32) | w1.x));
+                break;
+            }
+            case CLIFFT_OP_ARRAY_U2: array_u2(a1, p0); break;
+            case CLIFFT_OP_ARRAY_U4: array_u4(a1, a2, p0); break;
+            case CLIFFT_OP_EXPAND: expand(a1, false, 0.0, 0.0); break;
+            case CLIFFT_OP_EXPAND_T: expand(a1, true, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
+            case CLIFFT_OP_EXPAND_T_DAG: expand(a1, true, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
+            case CLIFFT_OP_EXPAND_ROT: {
+                const uint4 w1 = __ldg(ip + 2 * pc + 1);
+                expand(a1, true, __longlong_as_double(((long long)p1 << 32) | p0),
+                       __longlong_as_double(((long long)w1.y << 32) | w1.x));
+                break;
+            }
+            case CLIFFT_OP_MEAS_DORMANT_STATIC:
+                meas_dormant_static(a1, p0, sign, (fl & CLIFFT_FLAG_IDENTITY) != 0);
+                break;
+            case CLIFFT_OP_MEAS_DORMANT_RANDOM: meas_dormant_random(a1, p0, sign); break;
+            case CLIFFT_OP_MEAS_ACTIVE_DIAGONAL: meas_diagonal(a1, p0, sign); break;
+            case CLIFFT_OP_MEAS_ACTIVE_INTERFERE: meas_interfere(a1, a1, p0, sign); break;
+            case CLIFFT_OP_SWAP_MEAS_INTERFERE: meas_interfere(a1, a2, p0, sign); break;
+            case CLIFFT_OP_APPLY_PAULI:
+                flush_records();
+                if (bit_of(rec, p1, S))
+                    apply_pauli(P.pauli_x + (size_t)p0 * NW, P.pauli_z + (size_t)p0 * NW,
+                                P.pauli_sign[p0] != 0);
+                break;
+            case CLIFFT_OP_NOISE: noise(p0); break;
+            case CLIFFT_OP_NOISE_BLOCK:
+                while (next_noise >= p0 && next_noise - p0 < p1) noise(next_noise);
+                break;
+            case CLIFFT_OP_READOUT_NOISE: readout_noise(p0); break;
+            case CLIFFT_OP_DETECTOR: {
+                flush_records();
+                int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
+                par ^= list_parity(P.det_off, P.det_tg, p0);
+                if (Grp::rank() == 0 && par) det[(p1 >> 5) * S] |= 1u << (p1 & 31);
+                break;
+            }
+            case CLIFFT_OP_POSTSELECT: {
+                flush_records();
+                int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
+                par ^= list_parity(P.det_off, P.det_tg, p0);
+                if (par) {
+                    discarded = true;
+                    stop = true;
+                }
+                break;
+            }
+            case CLIFFT_OP_OBSERVABLE: {
+                flush_records();
+                int par = list_parity(P.obs_off, P.obs_tg, p0);
+                if (Grp::rank() == 0 && par) obs[(p1 >> 5) * S] ^= 1u << (p1 & 31);
+                break;
+            }
+            case CLIFFT_OP_EXP_VAL: exp_val(p0, p1); break;
+            default:
+                if (Grp::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_BAD_OPCODE);
+                stop = true;
+                break;
+        }
+    }
+
+    static __device__ __forceinline__ uint64_t pdep(uint64_t v, uint64_t mask) {
+        uint64_t r = 0;
+        for (uint64_t m = mask; m && v; m &= m - 1, v >>= 1)
+            if (v & 1u) r |= m & (~m + 1);
+        return r;
+    }
+
+    // Fused tile sweep starting at `pc` (CTA groups, statevector in global
+    // memory, k > tile bits). Returns the number of instructions consumed, 0
+    // when fewer than two sweeping opcodes would share the block.
+    __device__ uint32_t fused_block(uint32_t pc) {
+        constexpr uint32_t MB = TileCfg<R>::kBits;
+        constexpr uint32_t TN = 1u << MB;
+        uint64_t uni = 0;
+        int nsweep = 0;
+        uint32_t end = pc;
+        for (; end < P.n_instr; ++end) {
+            const uint4 w0 = __ldg(P.instr + 2 * end);
+            const uint32_t op = w0.x & 0xffu, x1 = w0.y & 0xffffu, x2 = w0.y >> 16;
+            uint64_t m = 0;
+            bool ok = true;
+            switch (op) {
+                case CLIFFT_OP_FRAME_CNOT:
+                case CLIFFT_OP_FRAME_CZ:
+                case CLIFFT_OP_FRAME_H:
+                case CLIFFT_OP_FRAME_S:
+                case CLIFFT_OP_FRAME_S_DAG:
+                case CLIFFT_OP_FRAME_SWAP: break;
+                case CLIFFT_OP_ARRAY_CNOT:
+                case CLIFFT_OP_ARRAY_CZ:
+                case CLIFFT_OP_ARRAY_SWAP:
+                case CLIFFT_OP_ARRAY_U4: m = (1ull << x1) | (1ull << x2); break;
+                case CLIFFT_OP_ARRAY_MULTI_CNOT:
+                case CLIFFT_OP_ARRAY_MULTI_CZ: m = (((uint64_t)w0.w << 32) | w0.z) | (1ull << x1); break;
+                case CLIFFT_OP_ARRAY_H:
+                case CLIFFT_OP_ARRAY_S:
+                case CLIFFT_OP_ARRAY_S_DAG: m = 1ull << x1; break;
+                case CLIFFT_OP_ARRAY_T:
+                case CLIFFT_OP_ARRAY_T_DAG:
+                case CLIFFT_OP_ARRAY_ROT:
+                case CLIFFT_OP_ARRAY_U2: m = x1 < k ? (1ull << x1) : 0ull; break;
+                default: ok = false;
+            }
+            if (!ok) break;
+            if (m) {
+                if ((uint32_t)__popcll(uni | m) > MB || nsweep >= kMaxMicroOps) break;
+                uni |= m;
+                nsweep++;
+            }
+        }
+        if (nsweep < 2) return 0;
+        // tile axes: the block's axes padded with the lowest free axes
+        uint64_t F = uni;
+        for (uint32_t a = 0; (uint32_t)__popcll(F) < MB; ++a) F |= 1ull << a;
+        const uint64_t C = ((k == 64) ? ~0ull : ((1ull << k) - 1)) & ~F;
+        uint8_t* lbit = reinterpret_cast<uint8_t*>(fuse + fuse_lbit_offset());
+        uint64_t* tlo = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
+        uint64_t* thi = tlo + 64;
+        if (Grp::rank() == 0) {
+            uint32_t j = 0;
+            for (uint32_t a = 0; a < k; ++a)
+                if ((F >> a) & 1u) lbit[a] = (uint8_t)j++;
+        }
+        if (Grp::rank() < 64) {
+            tlo[Grp::rank()] = pdep((uint64_t)Grp::rank(), F);
+            thi[Grp::rank()] = pdep((uint64_t)Grp::rank() << 6, F);
+        }
+        Grp::sync();
+        // resolve the block's frame-dependent choices into micro-ops
+        resolving = true;
+        n_mops = 0;
+        for (uint32_t q = pc; q < end; ++q) exec(q);
+        resolving = false;
+        Grp::sync();
+        // stream the statevector through shared memory, two tiles in flight
+        T* buf0 = reinterpret_cast<T*>(fuse);
+        T* buf1 = buf0 + TN;
+        const MicroOp* mops = reinterpret_cast<const MicroOp*>(fuse + fuse_mops_offset());
+        const uint64_t ntiles = 1ull << (k - MB);
+        const int tid = Grp::rank(), nthr = Grp::size();
+        auto issue = [&](uint64_t t, T* buf) {
+            const uint64_t base = pdep(t, C);
+            for (uint32_t l = tid; l < TN; l += nthr) {
+                const T* src = v + (base | tlo[l & 63u] | thi[l >> 6]);
+                if (sizeof(T) == 16)
+                    cp_async16(buf + l, src);
+                else
+                    cp_async8(buf + l, src);
+            }
+            cp_async_commit();
+        };
+        issue(0, buf0);
+        for (uint64_t t = 0; t < ntiles; ++t) {
+            T* cur = (t & 1) ? buf1 : buf0;
+            if (t + 1 < ntiles) {
+                issue(t + 1, (t & 1) ? buf0 : buf1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            Grp::sync();
+            for (int j = 0; j < n_mops; ++j) {
+                apply_micro(mops[j], cur, tid, nthr);
+                Grp::sync();
+            }
+            const uint64_t base = pdep(t, C);
+            for (uint32_t l = tid; l < TN; l += nthr) v[base | tlo[l & 63u] | thi[l >> 6]] = cur[l];
+            Grp::sync();
+        }
+        moved += (2ull << k) * sizeof(T);
+        return end - pc;
+    }
+
+    // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes; the
+    // arithmetic matches the unfused opcode handlers exactly.
+    static __device__ __forceinline__ void apply_micro(const MicroOp& m, T* tile, int tid, int nthr) {
+        constexpr uint32_t MB = TileCfg<R>::kBits;
+        const uint32_t a = m.a, b = m.b;
+        const uint32_t ab = 1u << a, bb = 1u << b;
+        switch (m.kind) {
+            case M_CNOT:
+                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
+                    uint32_t b0 = (uint32_t)ins00(i, a, b) | ab;
+                    T x = tile[b0];
+                    tile[b0] = tile[b0 | bb];
+                    tile[b0 | bb] = x;
+                }
+                break;
+            case M_CZ:
+                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
+                    uint32_t idx = (uint32_t)ins00(i, a, b) | ab | bb;
+                    tile[idx] = cneg(tile[idx]);
+                }
+                break;
+            case M_SWAP:
+                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
+                    uint32_t base = (uint32_t)ins00(i, a, b);
+                    T x = tile[base | ab];
+                    tile[base | ab] = tile[base | bb];
+                    tile[base | bb] = x;
+                }
+                break;
+            case M_MCNOT:
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    if (__popc(i0 & m.mask) & 1) {
+                        T x = tile[i0];
+                        tile[i0] = tile[i0 | ab];
+                        tile[i0 | ab] = x;
+                    }
+                }
+                break;
+            case M_MCZ:
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    uint32_t i0 = (uint32_t)ins0(i, a) | ab;
+                    if (__popc(i0 & m.mask) & 1) tile[i0] = cneg(tile[i0]);
+                }
+                break;
+            case M_H: {
+                const R s = (R)CGPU_INV_SQRT2;
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    T x = tile[i0], y = tile[i0 | ab];
+                    tile[i0] = cscale(cadd(x, y), s);
+                    tile[i0 | ab] = cscale(csub(x, y), s);
+                }
+                break;
+            }
+            case M_PHASE: {
+                const T ph = Cx<R>::make(m.c[0], m.c[1]);
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    uint32_t idx = (uint32_t)ins0(i, a) | ab;
+                    tile[idx] = cmul(tile[idx], ph);
+                }
+                break;
+            }
+            case M_U2: {
+                const T m00 = Cx<R>::make(m.c[0], m.c[1]), m01 = Cx<R>::make(m.c[2], m.c[3]);
+                const T m10 = Cx<R>::make(m.c[4], m.c[5]), m11 = Cx<R>::make(m.c[6], m.c[7]);
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    T x = tile[i0], y = tile[i0 | ab];
+                    tile[i0] = cadd(cmul(m00, x), cmul(m01, y));
+                    tile[i0 | ab] = cadd(cmul(m10, x), cmul(m11, y));
+                }
+                break;
+            }
+            case M_U4: {
+                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
+                    uint32_t q = (uint32_t)ins00(i, a, b);
+                    T x0 = tile[q], x1 = tile[q | ab], x2 = tile[q | bb], x3 = tile[q | ab | bb];
+                    T y[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const double* row = m.c + r * 8;
+                        T acc = cmul(Cx<R>::make(row[0], row[1]), x0);
+                        acc = cadd(acc, cmul(Cx<R>::make(row[2], row[3]), x1));
+                        acc = cadd(acc, cmul(Cx<R>::make(row[4], row[5]), x2));
+                        acc = cadd(acc, cmul(Cx<R>::make(row[6], row[7]), x3));
+                        y[r] = acc;
+                    }
+                    tile[q] = y[0];
+                    tile[q | ab] = y[1];
+                    tile[q | bb] = y[2];
+                    tile[q | ab | bb] = y[3];
+                }
+                break;
+            }
+            default: break;
+        }
+    }
+
     // ------------------------------------------------------------ driver
     __device__ __forceinline__ void run(Tally& tally) {
         // SchrodingerState::reset (svm_state.cc:220-267): only v[0] needs a
@@ -1043,6 +1468,9 @@ struct Shot {
         log_prob = 0.0;
         dust = 0;
         bytes = 0;
+        moved = 0;
+        resolving = false;
+        n_mops = 0;
         rec_dirty = false;
         forced = (K.flags & KF_FORCED_MEAS) ? K.forced_meas + shot * P.slots : nullptr;
         meas_prob = (K.flags & KF_TRACE) && K.out_meas_prob ? K.out_meas_prob + shot * P.slots : nullptr;
@@ -1068,104 +1496,17 @@ struct Shot {
         }
         Grp::sync();
 
-        const uint4* ip = P.instr;
         const uint32_t n_instr = P.n_instr;
+        const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) && fuse != nullptr;
         for (uint32_t pc = 0; pc < n_instr; ++pc) {
-            const uint4 w0 = __ldg(ip + 2 * pc);
-            uint32_t op = w0.x & 0xffu;
-            const uint32_t fl = (w0.x >> 16) & 0xffu;
-            const uint32_t a1 = w0.y & 0xffffu, a2 = w0.y >> 16;
-            const uint32_t p0 = w0.z, p1 = w0.w;
-            const int sign = (fl & CLIFFT_FLAG_SIGN) ? 1 : 0;
-            if (op >= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED)
-                op -= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED - CLIFFT_OP_MEAS_DORMANT_STATIC;
-            switch (op) {
-                case CLIFFT_OP_FRAME_CNOT: frame_cnot(a1, a2); break;
-                case CLIFFT_OP_FRAME_CZ: frame_cz(a1, a2); break;
-                case CLIFFT_OP_FRAME_H: frame_h(a1); break;
-                case CLIFFT_OP_FRAME_S: frame_s(a1, false); break;
-                case CLIFFT_OP_FRAME_S_DAG: frame_s(a1, true); break;
-                case CLIFFT_OP_FRAME_SWAP: frame_swap(a1, a2); break;
-                case CLIFFT_OP_ARRAY_CNOT: array_cnot(a1, a2); break;
-                case CLIFFT_OP_ARRAY_CZ: array_cz(a1, a2); break;
-                case CLIFFT_OP_ARRAY_SWAP: array_swap(a1, a2); break;
-                case CLIFFT_OP_ARRAY_MULTI_CNOT: array_multi_cnot(a1, ((uint64_t)p1 << 32) | p0); break;
-                case CLIFFT_OP_ARRAY_MULTI_CZ: array_multi_cz(a1, ((uint64_t)p1 << 32) | p0); break;
-                case CLIFFT_OP_ARRAY_H: array_h(a1); break;
-                case CLIFFT_OP_ARRAY_S:
-                    phase_sweep(a1, 0.0, 1.0);
-                    frame_s(a1, false);
-                    break;
-                case CLIFFT_OP_ARRAY_S_DAG:
-                    phase_sweep(a1, 0.0, -1.0);
-                    frame_s(a1, true);
-                    break;
-                case CLIFFT_OP_ARRAY_T: array_rot(a1, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_ARRAY_T_DAG: array_rot(a1, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_ARRAY_ROT: {
-                    const uint4 w1 = __ldg(ip + 2 * pc + 1);
-                    array_rot(a1, __longlong_as_double(((long long)p1 << 32) | p0),
-                              __longlong_as_double(((long long)w1.y << 32) | w1.x));
-                    break;
+            if (fuse_on && k > TileCfg<R>::kBits) {
+                const uint32_t used = fused_block(pc);
+                if (used) {
+                    pc += used - 1;
+                    continue;
                 }
-                case CLIFFT_OP_ARRAY_U2: array_u2(a1, p0); break;
-                case CLIFFT_OP_ARRAY_U4: array_u4(a1, a2, p0); break;
-                case CLIFFT_OP_EXPAND: expand(a1, false, 0.0, 0.0); break;
-                case CLIFFT_OP_EXPAND_T: expand(a1, true, CGPU_INV_SQRT2, CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_EXPAND_T_DAG: expand(a1, true, CGPU_INV_SQRT2, -CGPU_INV_SQRT2); break;
-                case CLIFFT_OP_EXPAND_ROT: {
-                    const uint4 w1 = __ldg(ip + 2 * pc + 1);
-                    expand(a1, true, __longlong_as_double(((long long)p1 << 32) | p0),
-                           __longlong_as_double(((long long)w1.y << 32) | w1.x));
-                    break;
-                }
-                case CLIFFT_OP_MEAS_DORMANT_STATIC:
-                    meas_dormant_static(a1, p0, sign, (fl & CLIFFT_FLAG_IDENTITY) != 0);
-                    break;
-                case CLIFFT_OP_MEAS_DORMANT_RANDOM: meas_dormant_random(a1, p0, sign); break;
-                case CLIFFT_OP_MEAS_ACTIVE_DIAGONAL: meas_diagonal(a1, p0, sign); break;
-                case CLIFFT_OP_MEAS_ACTIVE_INTERFERE: meas_interfere(a1, a1, p0, sign); break;
-                case CLIFFT_OP_SWAP_MEAS_INTERFERE: meas_interfere(a1, a2, p0, sign); break;
-                case CLIFFT_OP_APPLY_PAULI:
-                    flush_records();
-                    if (bit_of(rec, p1, S))
-                        apply_pauli(P.pauli_x + (size_t)p0 * NW, P.pauli_z + (size_t)p0 * NW,
-                                    P.pauli_sign[p0] != 0);
-                    break;
-                case CLIFFT_OP_NOISE: noise(p0); break;
-                case CLIFFT_OP_NOISE_BLOCK:
-                    while (next_noise >= p0 && next_noise - p0 < p1) noise(next_noise);
-                    break;
-                case CLIFFT_OP_READOUT_NOISE: readout_noise(p0); break;
-                case CLIFFT_OP_DETECTOR: {
-                    flush_records();
-                    int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
-                    par ^= list_parity(P.det_off, P.det_tg, p0);
-                    if (Grp::rank() == 0 && par) det[(p1 >> 5) * S] |= 1u << (p1 & 31);
-                    break;
-                }
-                case CLIFFT_OP_POSTSELECT: {
-                    flush_records();
-                    int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
-                    par ^= list_parity(P.det_off, P.det_tg, p0);
-                    if (par) {
-                        discarded = true;
-                        stop = true;
-                    }
-                    break;
-                }
-                case CLIFFT_OP_OBSERVABLE: {
-                    flush_records();
-                    int par = list_parity(P.obs_off, P.obs_tg, p0);
-                    if (Grp::rank() == 0 && par) obs[(p1 >> 5) * S] ^= 1u << (p1 & 31);
-                    break;
-                }
-                case CLIFFT_OP_EXP_VAL: exp_val(p0, p1); break;
-                default:
-                    if (Grp::rank() == 0) atomicCAS(K.error_word, 0, DEV_ERR_BAD_OPCODE);
-                    stop = true;
-                    break;
             }
+            exec(pc);
             if (stop) break;
         }
         Grp::sync();
@@ -1223,12 +1564,13 @@ struct Shot {
                 for (uint32_t i = 0; i < P.num_obs; ++i)
                     if ((obs[(i >> 5) * S] >> (i & 31)) & 1u) {
                         any = true;
-                        atomicAdd(K.counters + 4 + i, 1ull);
+                        atomicAdd(K.counters + 5 + i, 1ull);
                     }
                 if (any) tally.logical++;
             }
             tally.dust += dust;
             tally.bytes += bytes;
+            tally.moved += moved;
         }
         if (K.out_final_v && shot < K.dump_shots) {
             const uint64_t stride = 1ull << P.peak, n = 1ull << k;
@@ -1259,7 +1601,7 @@ __host__ __device__ constexpr int shots_per_group_region() {
 }
 
 template <typename R, int G, int NW>
-__global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const DevProg P, const KParams K) {
+__global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample_kernel(const DevProg P, const KParams K) {
     using Grp = typename GroupOf<G>::type;
     using T = typename Cx<R>::T;
     constexpr int S = Grp::S;
@@ -1267,8 +1609,8 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const
     const int region = Grp::kCta ? 0 : (int)(threadIdx.x >> 5);
     const int regions = Grp::kCta ? 1 : (int)(blockDim.x >> 5);
     const size_t state_bytes = K.state_in_smem ? (size_t)K.state_stride * S * sizeof(T) : 0;
-    const size_t rec_bytes = (size_t)(K.rec_words + K.det_words + K.obs_words) * S * 4;
-    const size_t region_bytes = (state_bytes + rec_bytes + 15) & ~(size_t)15;
+    const size_t rec_bytes = ((size_t)(K.rec_words + K.det_words + K.obs_words) * S * 4 + 15) & ~(size_t)15;
+    const size_t region_bytes = (state_bytes + rec_bytes + K.fuse_bytes + 15) & ~(size_t)15;
     unsigned char* rbase = smem + (size_t)region * region_bytes;
     unsigned char* tail = smem + (size_t)regions * region_bytes;
     double* red = reinterpret_cast<double*>(tail);
@@ -1277,6 +1619,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const
     uint32_t* rec = reinterpret_cast<uint32_t*>(rbase + state_bytes) + Grp::slot();
     uint32_t* det = rec + (size_t)K.rec_words * S;
     uint32_t* obs = det + (size_t)K.det_words * S;
+    unsigned char* fz = K.fuse_bytes ? rbase + state_bytes + rec_bytes : nullptr;
     T* v;
     if (K.state_in_smem) {
         v = reinterpret_cast<T*>(rbase) + Grp::slot();
@@ -1299,7 +1642,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const
         if (base >= K.shots) break;
         const unsigned long long shot = base + Grp::slot();
         if (shot < K.shots) {
-            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, shot);
+            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, fz, shot);
             s.run(tally);
         }
         if (!Grp::kCta) __syncwarp();
@@ -1309,6 +1652,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 256, 1) svm_sample_kernel(const
     if (tally.logical) atomicAdd(K.counters + 1, tally.logical);
     if (tally.dust) atomicAdd(K.counters + 2, tally.dust);
     if (tally.bytes) atomicAdd(K.counters + 3, tally.bytes);
+    if (tally.moved) atomicAdd(K.counters + 4, tally.moved);
 }
 
 }  // namespace cgpu

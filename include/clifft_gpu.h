@@ -60,6 +60,7 @@ extern "C" {
 #define CLIFFT_GPU_FORCED_FAULTS 0x04u  /* fault sites / channels / readout flips from the CSR inputs */
 #define CLIFFT_GPU_DEVICE_PTRS 0x08u    /* every input/output pointer is a device pointer */
 #define CLIFFT_GPU_TRACE 0x10u          /* fill meas_prob and the final-state dump */
+#define CLIFFT_GPU_NO_FUSION 0x20u      /* plain executor: one statevector sweep per opcode */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
 
@@ -106,11 +107,13 @@ typedef struct clifft_gpu_outputs {
     uint64_t logical_errors;
     uint64_t* observable_ones; /* num_observables counters, may be NULL */
     uint64_t dust_clamps;
-    uint64_t algorithmic_bytes; /* statevector bytes the executed opcodes must move (read + write) */
+    uint64_t algorithmic_bytes; /* statevector bytes the executed opcodes must move, opcode by opcode */
+    uint64_t streamed_bytes;    /* statevector bytes actually streamed (a fused block streams once) */
     uint32_t kernel_launches;  /* kernels this call launched */
     float kernel_ms;           /* device time of the sampling kernel(s) */
     uint32_t group_threads;    /* shot-group size that ran */
     uint32_t state_in_smem;    /* 1 if the statevectors lived in shared memory */
+    uint32_t fused;            /* 1 if fused tile sweeps were enabled */
 } clifft_gpu_outputs;
 
 /* Upload + validate a program. *out receives an opaque handle. */

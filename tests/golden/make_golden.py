@@ -43,6 +43,8 @@ def cases():
                                                       postselect=(seed % 4 == 3))))
     out.append(("fuzz_k9", random_program(100, n=12, length=260, max_k=9)))
     out.append(("fuzz_w2", random_program(101, n=70, length=200, max_k=6)))
+    out.append(("fuzz_k16", random_program(102, n=24, length=260, max_k=16, noise=True,
+                                           expand_bias=0.45)))
     out.append(("cfg0", W.lower(W.config0())))
     c2 = W.config2_circuits()
     out.append(("cfg2_s105", W.lower(c2[5])))
@@ -57,6 +59,7 @@ def main():
         raise SystemExit("reference harness missing: run oracle/build_ref.sh first")
     for name, raw in cases():
         prog = O.ref_passes(raw, O.PASS_ALL)
+        shots_forced = 6 if prog.peak_rank > 12 else FORCED_SHOTS
         prog.name = name
         d = {f"prog_{k}": v for k, v in prog.to_npz_dict().items()}
         d["ref_backend"] = np.array(O.ref_backend())
@@ -71,21 +74,21 @@ def main():
         # forced inputs: random faults and readout flips, and outcomes sampled
         # by the oracle under those same faults (every 5th record flipped to
         # exercise unreachable outcomes)
-        faults, ros = random_forced_inputs(prog, FORCED_SHOTS, seed + 2, fault_rate=0.2)
-        o = O.run(prog, FORCED_SHOTS, seed=seed + 1, rng=O.RNG_PHILOX, faults=faults,
+        faults, ros = random_forced_inputs(prog, shots_forced, seed + 2, fault_rate=0.2)
+        o = O.run(prog, shots_forced, seed=seed + 1, rng=O.RNG_PHILOX, faults=faults,
                   readout_faults=ros)
-        fm = np.zeros((FORCED_SHOTS, prog.total_meas_slots), np.uint8)
+        fm = np.zeros((shots_forced, prog.total_meas_slots), np.uint8)
         fm[:, :prog.num_measurements] = o["meas"]
         fm[::5] ^= 1
         f = O.ref_forced(prog, fm, faults, ros)
         d["forced_meas_in"] = fm
-        fo = np.zeros(FORCED_SHOTS + 1, np.uint32)
+        fo = np.zeros(shots_forced + 1, np.uint32)
         flat_s, flat_c = [], []
         for i, sh in enumerate(faults):
             flat_s += [x[0] for x in sh]
             flat_c += [x[1] for x in sh]
             fo[i + 1] = len(flat_s)
-        ro = np.zeros(FORCED_SHOTS + 1, np.uint32)
+        ro = np.zeros(shots_forced + 1, np.uint32)
         flat_r = []
         for i, sh in enumerate(ros):
             flat_r += sh
@@ -95,6 +98,9 @@ def main():
                  readout_entries=np.array(flat_r, np.uint32))
         for k, v in f.items():
             d[f"forced_{k}"] = v
+        if prog.peak_rank > 12:
+            # large statevectors: keep the first 2^12 amplitudes of each final state
+            d["forced_final_v"] = f["final_v"][:, :1 << 12]
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **d)
         print(name, prog.summary()["ops"].get("ARRAY_U2", 0), prog.summary()["ops"].get("ARRAY_U4", 0),
               prog.peak_rank, prog.num_instructions)
