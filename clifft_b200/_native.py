@@ -22,6 +22,7 @@ CLIFFT_GPU_FORCED_FAULTS = 0x04
 CLIFFT_GPU_DEVICE_PTRS = 0x08
 CLIFFT_GPU_TRACE = 0x10
 CLIFFT_GPU_NO_FUSION = 0x20
+CLIFFT_GPU_FORCE_FUSION = 0x40
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device error", -4: "out of memory"}
 

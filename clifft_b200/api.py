@@ -86,9 +86,11 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         faults: Optional[Sequence[Sequence[tuple]]] = None,
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
-        dust_eps: float = 0.0, want_records: bool = True, fusion: bool = True) -> Dict[str, object]:
+        dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
-    records plus everything the call reports."""
+    records plus everything the call reports. `fusion`: None = automatic (fused
+    tile sweeps when global-memory statevectors outgrow L2), True = always
+    fuse, False = one sweep per opcode (the plain executor)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:
@@ -121,8 +123,10 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_FORCED_FAULTS
     if trace:
         flags |= N.CLIFFT_GPU_TRACE
-    if not fusion:
+    if fusion is False:
         flags |= N.CLIFFT_GPU_NO_FUSION
+    elif fusion is True:
+        flags |= N.CLIFFT_GPU_FORCE_FUSION
     a.flags = flags
     o = N.Outputs()
     if want_records:

@@ -568,6 +568,15 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const uint32_t obs_words = (m.num_observables + 31) / 32;
         LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words,
                                    det_words, obs_words, (args->flags & CLIFFT_GPU_NO_FUSION) == 0);
+        if (L.fuse && !(args->flags & CLIFFT_GPU_FORCE_FUSION)) {
+            // Statevectors that stay resident in L2 sweep faster opcode by
+            // opcode; fuse only when the resident set streams from HBM.
+            const size_t amp_b = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
+            const uint64_t resident = uint64_t(L.blocks) * L.regions * L.S * L.state_stride * amp_b;
+            if (resident < (uint64_t(96) << 20))
+                L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words, det_words,
+                                obs_words, false);
+        }
 
         KParams K{};
         K.shots = shots;

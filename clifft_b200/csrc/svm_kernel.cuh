@@ -152,32 +152,46 @@ struct Cx<double> {
     static __device__ __forceinline__ T make(double re, double im) { return make_double2(re, im); }
 };
 
+// Complex arithmetic with every rounding step spelled out (explicit fma and
+// round-to-nearest products / sums), so the compiler cannot contract
+// differently in different inlining contexts: the fused tile path, the
+// per-opcode sweeps and every launch shape perform bit-identical arithmetic.
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float rn_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double rn_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 template <typename T>
 __device__ __forceinline__ T cadd(T a, T b) {
     T r;
-    r.x = a.x + b.x;
-    r.y = a.y + b.y;
+    r.x = rn_add(a.x, b.x);
+    r.y = rn_add(a.y, b.y);
     return r;
 }
 template <typename T>
 __device__ __forceinline__ T csub(T a, T b) {
     T r;
-    r.x = a.x - b.x;
-    r.y = a.y - b.y;
+    r.x = rn_sub(a.x, b.x);
+    r.y = rn_sub(a.y, b.y);
     return r;
 }
+// (a.x b.x - a.y b.y, a.x b.y + a.y b.x): one rounded product, one fma per part
 template <typename T>
 __device__ __forceinline__ T cmul(T a, T b) {
     T r;
-    r.x = a.x * b.x - a.y * b.y;
-    r.y = a.x * b.y + a.y * b.x;
+    r.x = rn_fma(a.x, b.x, -rn_mul(a.y, b.y));
+    r.y = rn_fma(a.x, b.y, rn_mul(a.y, b.x));
     return r;
 }
 template <typename T, typename S>
 __device__ __forceinline__ T cscale(T a, S s) {
     T r;
-    r.x = a.x * s;
-    r.y = a.y * s;
+    r.x = rn_mul(a.x, s);
+    r.y = rn_mul(a.y, s);
     return r;
 }
 template <typename T>
@@ -190,10 +204,10 @@ __device__ __forceinline__ T cneg(T a) {
 template <typename T>
 __device__ __forceinline__ double cnorm_d(T a) {
     double x = (double)a.x, y = (double)a.y;
-    return x * x + y * y;
+    return __fma_rn(x, x, __dmul_rn(y, y));
 }
 __device__ __forceinline__ double2 dmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_double2(__fma_rn(a.x, b.x, -__dmul_rn(a.y, b.y)), __fma_rn(a.x, b.y, __dmul_rn(a.y, b.x)));
 }
 
 // kInvSqrt2 = std::numbers::sqrt2 / 2 (src/clifft/util/constants.h) and the
@@ -1123,12 +1137,12 @@ struct Shot {
                     if (j < dim) {
                         double ar = (double)av[u].x, ai = (double)av[u].y;
                         double br = (double)bv[u].x, bi = -(double)bv[u].y;
-                        acc[2] += ar * ar + ai * ai;
+                        acc[2] = __dadd_rn(acc[2], __fma_rn(ar, ar, __dmul_rn(ai, ai)));
                         double zs = (__popcll(j & za) & 1) ? -1.0 : 1.0;
                         ar *= zs;
                         ai *= zs;
-                        acc[0] += br * ar - bi * ai;
-                        acc[1] += br * ai + bi * ar;
+                        acc[0] = __dadd_rn(acc[0], __fma_rn(br, ar, -__dmul_rn(bi, ai)));
+                        acc[1] = __dadd_rn(acc[1], __fma_rn(br, ai, __dmul_rn(bi, ar)));
                     }
                 }
             }
