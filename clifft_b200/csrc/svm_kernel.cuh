@@ -134,6 +134,7 @@ enum : uint32_t {
 enum : int {
     DEV_ERR_ZERO_NORM = 1,
     DEV_ERR_BAD_OPCODE = 2,
+    DEV_ERR_TIMEOUT = 3,  // a bounded wait on a bulk-copy barrier gave up
 };
 
 // ----------------------------------------------------------------- complex
@@ -379,15 +380,54 @@ struct MicroOp {
     double c[32];   // up to 16 complex coefficients
 };
 constexpr int kMaxMicroOps = 24;
+constexpr int kStages = 4;         // tiles in flight per CTA
+constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 template <typename R>
 struct TileCfg {
     static constexpr int kBits = sizeof(R) == 4 ? 12 : 11;  // 32 KiB per tile buffer
 };
 template <typename R>
 __host__ __device__ constexpr uint32_t fuse_smem_bytes() {
-    return (uint32_t)(2u * (1u << TileCfg<R>::kBits) * 2u * sizeof(R) + kMaxMicroOps * sizeof(MicroOp) +
-                      2u * 64u * 8u + 64u);
+    return (uint32_t)(kStages * (1u << TileCfg<R>::kBits) * 2u * sizeof(R) + kStages * 8u +
+                      kMaxMicroOps * sizeof(MicroOp) + 64u * 8u + 64u + 64u);
 }
+
+// ---- bulk-copy (TMA, untiled) and mbarrier primitives. Every copy here reads
+// or writes this GPU's own global memory; none uses cluster multicast.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok;
+}
+__device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst_smem)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* dst, const void* src_smem, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src_smem)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -555,13 +595,16 @@ struct Shot {
     __device__ __forceinline__ uint8_t local_bit(uint32_t axis) const {
         return reinterpret_cast<const uint8_t*>(fuse + fuse_lbit_offset())[axis];
     }
-    static __host__ __device__ constexpr uint32_t fuse_mops_offset() {
-        return 2u * (1u << TileCfg<R>::kBits) * (uint32_t)sizeof(T);
+    // fused-sweep scratch: [kStages tile buffers][kStages mbarriers][micro-ops]
+    // [64 run offsets][64-byte axis -> local bit table]
+    static __host__ __device__ constexpr uint32_t fuse_bar_offset() {
+        return kStages * (1u << TileCfg<R>::kBits) * (uint32_t)sizeof(T);
     }
+    static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return fuse_bar_offset() + kStages * 8u; }
     static __host__ __device__ constexpr uint32_t fuse_tables_offset() {
         return fuse_mops_offset() + kMaxMicroOps * (uint32_t)sizeof(MicroOp);
     }
-    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return fuse_tables_offset() + 2u * 64u * 8u; }
+    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return fuse_tables_offset() + 64u * 8u; }
     __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
                                          int nc) {
         if (Grp::rank() == 0) {
@@ -1263,12 +1306,105 @@ struct Shot {
         return r;
     }
 
-    // Fused tile sweep starting at `pc` (CTA groups, statevector in global
-    // memory, k > tile bits). Returns the number of instructions consumed, 0
-    // when fewer than two sweeping opcodes would share the block.
-    __device__ uint32_t fused_block(uint32_t pc) {
+    // Tile axes for a set of axes `uni` (|uni| < TILE_BITS): `uni` padded with
+    // the lowest free axes. Returns F and sets `r` to the length (log2) of the
+    // contiguous low run, so one tile is 2^(TILE_BITS - r) runs of 2^r
+    // consecutive amplitudes.
+    __device__ __forceinline__ uint64_t tile_axes(uint64_t uni, uint32_t& r) const {
+        constexpr uint32_t MB = TileCfg<R>::kBits;
+        uint64_t F = uni;
+        for (uint32_t a = 0; (uint32_t)__popcll(F) < MB; ++a) F |= 1ull << a;
+        r = (uint32_t)__ffsll((long long)~F) - 1;  // count of consecutive low axes in F
+        return F;
+    }
+
+    // One streamed pass over 2^(k_pass) amplitudes in tiles of 2^TILE_BITS:
+    // tile t covers the run offsets `runoff` (shared table, 2^(TILE_BITS - r)
+    // runs of 2^r amplitudes) shifted by pdep(t, C). Loads come from
+    // v[load_add + ...], optional stores (the first `store_runs` runs of each
+    // tile) go to v[store_add + ...]. Bulk copies (TMA) run kStages tiles
+    // ahead; `compute(buf, t)` is called by every thread and must synchronise
+    // the CTA before it returns. Returns false after a barrier timeout.
+    template <class Compute>
+    __device__ bool stream_tiles(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add, uint64_t store_add,
+                                 uint32_t store_runs, Compute compute) {
         constexpr uint32_t MB = TileCfg<R>::kBits;
         constexpr uint32_t TN = 1u << MB;
+        T* bufs = reinterpret_cast<T*>(fuse);
+        uint64_t* bars = reinterpret_cast<uint64_t*>(fuse + fuse_bar_offset());
+        const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
+        const uint32_t nruns = 1u << (MB - r);
+        const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
+        const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+        // statevector writes made by ordinary stores must be visible to the copy engine
+        fence_async_global();
+        if (tid == 0) {
+            for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        auto issue_load = [&](uint64_t t) {
+            const uint32_t st = (uint32_t)(t % kStages);
+            const uint64_t base = load_add + pdep(t, C);
+            if (lane == 0) mbar_expect_tx(&bars[st], TN * (uint32_t)sizeof(T));
+            __syncwarp();
+            for (uint32_t j = lane; j < nruns; j += 32)
+                bulk_load(bufs + st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[st]);
+        };
+        if (warp == 0)
+            for (uint64_t t = 0; t < ntiles && t < (uint64_t)(kStages - 1); ++t) issue_load(t);
+        bool ok_all = true;
+        uint64_t t = 0;
+        for (; t < ntiles; ++t) {
+            const uint32_t st = (uint32_t)(t % kStages);
+            const uint32_t parity = (uint32_t)((t / kStages) & 1u);
+            uint32_t ok = 0;
+            for (uint32_t it = 0; it < (1u << 20) && !ok; ++it) ok = mbar_try_wait(&bars[st], parity);
+            if (__syncthreads_or(!ok)) {
+                ok_all = false;
+                break;
+            }
+            T* buf = bufs + st * TN;
+            compute(buf, t);
+            if (store_runs) {
+                fence_async_shared();
+                __syncthreads();
+                if (warp == 0) {
+                    const uint64_t base = store_add + pdep(t, C);
+                    for (uint32_t j = lane; j < store_runs; j += 32)
+                        bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
+                    bulk_commit();
+                }
+            }
+            if (warp == 0 && t + kStages - 1 < ntiles) {
+                if (store_runs) bulk_wait_read1();  // the stage being refilled held tile t-1
+                __syncwarp();
+                issue_load(t + kStages - 1);
+            }
+        }
+        if (!ok_all) {
+            // drain (bounded) every load still in flight before the buffers go away
+            if (tid == 0) atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT);
+            for (uint64_t q = t; q < ntiles && q < t + kStages - 1; ++q) {
+                const uint32_t st = (uint32_t)(q % kStages);
+                for (uint32_t it = 0; it < (1u << 20); ++it)
+                    if (mbar_try_wait(&bars[st], (uint32_t)((q / kStages) & 1u))) break;
+            }
+            stop = true;
+        }
+        if (warp == 0) {
+            bulk_wait_all();
+            fence_async_global();
+        }
+        __syncthreads();
+        return ok_all;
+    }
+
+    // Fused tile sweep starting at `pc` (CTA groups, statevector in global
+    // memory, k > tile bits). Returns the number of instructions consumed, 0
+    // when the opcode at `pc` cannot start a block.
+    __device__ uint32_t fused_block(uint32_t pc) {
+        constexpr uint32_t MB = TileCfg<R>::kBits;
         uint64_t uni = 0;
         int nsweep = 0;
         uint32_t end = pc;
@@ -1301,28 +1437,27 @@ struct Shot {
             }
             if (!ok) break;
             if (m) {
-                if ((uint32_t)__popcll(uni | m) > MB || nsweep >= kMaxMicroOps) break;
-                uni |= m;
+                const uint64_t cand = uni | m;
+                uint32_t rr;
+                if ((uint32_t)__popcll(cand) >= MB || nsweep >= kMaxMicroOps) break;
+                tile_axes(cand, rr);
+                if (MB - rr > (uint32_t)kMaxRunsLog2) break;
+                uni = cand;
                 nsweep++;
             }
         }
-        if (nsweep < 2) return 0;
-        // tile axes: the block's axes padded with the lowest free axes
-        uint64_t F = uni;
-        for (uint32_t a = 0; (uint32_t)__popcll(F) < MB; ++a) F |= 1ull << a;
+        if (nsweep < 1) return 0;
+        uint32_t r;
+        const uint64_t F = tile_axes(uni, r);
         const uint64_t C = ((k == 64) ? ~0ull : ((1ull << k) - 1)) & ~F;
         uint8_t* lbit = reinterpret_cast<uint8_t*>(fuse + fuse_lbit_offset());
-        uint64_t* tlo = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
-        uint64_t* thi = tlo + 64;
+        uint64_t* runoff = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
         if (Grp::rank() == 0) {
             uint32_t j = 0;
             for (uint32_t a = 0; a < k; ++a)
                 if ((F >> a) & 1u) lbit[a] = (uint8_t)j++;
         }
-        if (Grp::rank() < 64) {
-            tlo[Grp::rank()] = pdep((uint64_t)Grp::rank(), F);
-            thi[Grp::rank()] = pdep((uint64_t)Grp::rank() << 6, F);
-        }
+        if (Grp::rank() < (1 << (MB - r))) runoff[Grp::rank()] = pdep((uint64_t)Grp::rank() << r, F);
         Grp::sync();
         // resolve the block's frame-dependent choices into micro-ops
         resolving = true;
@@ -1330,41 +1465,15 @@ struct Shot {
         for (uint32_t q = pc; q < end; ++q) exec(q);
         resolving = false;
         Grp::sync();
-        // stream the statevector through shared memory, two tiles in flight
-        T* buf0 = reinterpret_cast<T*>(fuse);
-        T* buf1 = buf0 + TN;
         const MicroOp* mops = reinterpret_cast<const MicroOp*>(fuse + fuse_mops_offset());
-        const uint64_t ntiles = 1ull << (k - MB);
         const int tid = Grp::rank(), nthr = Grp::size();
-        auto issue = [&](uint64_t t, T* buf) {
-            const uint64_t base = pdep(t, C);
-            for (uint32_t l = tid; l < TN; l += nthr) {
-                const T* src = v + (base | tlo[l & 63u] | thi[l >> 6]);
-                if (sizeof(T) == 16)
-                    cp_async16(buf + l, src);
-                else
-                    cp_async8(buf + l, src);
+        const int nm = n_mops;
+        stream_tiles(1ull << (k - MB), C, r, 0, 0, 1u << (MB - r), [&](T* buf, uint64_t) {
+            for (int j = 0; j < nm; ++j) {
+                apply_micro(mops[j], buf, tid, nthr);
+                __syncthreads();
             }
-            cp_async_commit();
-        };
-        issue(0, buf0);
-        for (uint64_t t = 0; t < ntiles; ++t) {
-            T* cur = (t & 1) ? buf1 : buf0;
-            if (t + 1 < ntiles) {
-                issue(t + 1, (t & 1) ? buf0 : buf1);
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
-            }
-            Grp::sync();
-            for (int j = 0; j < n_mops; ++j) {
-                apply_micro(mops[j], cur, tid, nthr);
-                Grp::sync();
-            }
-            const uint64_t base = pdep(t, C);
-            for (uint32_t l = tid; l < TN; l += nthr) v[base | tlo[l & 63u] | thi[l >> 6]] = cur[l];
-            Grp::sync();
-        }
+        });
         moved += (2ull << k) * sizeof(T);
         return end - pc;
     }
