@@ -23,6 +23,7 @@ CLIFFT_GPU_DEVICE_PTRS = 0x08
 CLIFFT_GPU_TRACE = 0x10
 CLIFFT_GPU_NO_FUSION = 0x20
 CLIFFT_GPU_FORCE_FUSION = 0x40
+CLIFFT_GPU_PROFILE = 0x80
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device error", -4: "out of memory"}
 
@@ -50,7 +51,7 @@ class Outputs(ctypes.Structure):
         ("algorithmic_bytes", ctypes.c_uint64), ("streamed_bytes", ctypes.c_uint64),
         ("kernel_launches", ctypes.c_uint32), ("kernel_ms", ctypes.c_float),
         ("group_threads", ctypes.c_uint32), ("state_in_smem", ctypes.c_uint32),
-        ("fused", ctypes.c_uint32),
+        ("fused", ctypes.c_uint32), ("phase_cycles", ctypes.c_uint64 * 5),
     ]
 
 

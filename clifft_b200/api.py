@@ -86,7 +86,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         faults: Optional[Sequence[Sequence[tuple]]] = None,
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
-        dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None) -> Dict[str, object]:
+        dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
+        profile: bool = False) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None = automatic (fused
     tile sweeps when global-memory statevectors outgrow L2), True = always
@@ -123,6 +124,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_FORCED_FAULTS
     if trace:
         flags |= N.CLIFFT_GPU_TRACE
+    if profile:
+        flags |= N.CLIFFT_GPU_PROFILE
     if fusion is False:
         flags |= N.CLIFFT_GPU_NO_FUSION
     elif fusion is True:
@@ -163,7 +166,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
     res.update(passed_shots=int(o.passed_shots), logical_errors=int(o.logical_errors),
                observable_ones=ones[:p.num_observables].copy(), dust_clamps=int(o.dust_clamps),
                algorithmic_bytes=int(o.algorithmic_bytes), streamed_bytes=int(o.streamed_bytes),
-               fused=bool(o.fused),
+               fused=bool(o.fused), phase_cycles=list(o.phase_cycles),
                kernel_ms=float(o.kernel_ms), kernel_launches=int(o.kernel_launches),
                group_threads=int(o.group_threads), state_in_smem=bool(o.state_in_smem))
     return res

@@ -332,7 +332,8 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
                ~size_t(15);
     };
-    auto tail = [&](int threads) { return size_t(3 * 8 * (threads / 32) + 64); };
+    // block tail: reduction scratch for up to 32 warps, broadcast slot, control state
+    auto tail = [&](int threads) { (void)threads; return size_t(3 * 8 * 32 + 64 + kCtlBytes); };
     if (G) {
         L.threads = std::min(128, max_threads);
         L.regions = L.threads / 32;
@@ -601,8 +602,11 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         if (!L.state_in_smem)
             K.state_global = buf.alloc(size_t(L.blocks) * L.regions * L.S * L.state_stride * amp);
         const size_t n_counters = 5 + m.num_observables;
-        auto* scratch = static_cast<unsigned long long*>(buf.alloc((2 + n_counters) * 8 + 64));
-        CUDA_OK(cudaMemsetAsync(scratch, 0, (2 + n_counters) * 8 + 64, st));
+        const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;
+        const size_t scratch_words = 2 + n_counters + (profile ? 8 : 0);
+        auto* scratch = static_cast<unsigned long long*>(buf.alloc(scratch_words * 8 + 64));
+        CUDA_OK(cudaMemsetAsync(scratch, 0, scratch_words * 8 + 64, st));
+        K.phase_cycles = profile ? scratch + 2 + n_counters : nullptr;
         K.work_counter = scratch;
         K.error_word = reinterpret_cast<int*>(scratch + 1);
         K.counters = scratch + 2;
@@ -675,7 +679,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         CUDA_OK(cudaEventRecord(e1, st));
 
         for (auto& o : outs) CUDA_OK(cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, st));
-        std::vector<unsigned long long> hs(2 + n_counters);
+        std::vector<unsigned long long> hs(scratch_words);
         CUDA_OK(cudaMemcpyAsync(hs.data(), scratch, hs.size() * 8, cudaMemcpyDeviceToHost, st));
         std::vector<uint64_t> hpx, hpz;
         const uint32_t nwt = L.nw_words;
@@ -715,6 +719,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->group_threads = L.G ? uint32_t(L.G) : uint32_t(L.threads);
         out->state_in_smem = L.state_in_smem ? 1u : 0u;
         out->fused = L.fuse ? 1u : 0u;
+        for (int i = 0; i < 5; ++i) out->phase_cycles[i] = profile ? hs[2 + n_counters + i] : 0;
     });
 }
 

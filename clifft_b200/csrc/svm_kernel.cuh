@@ -121,6 +121,7 @@ struct KParams {
     double* out_final_v;
     uint64_t dump_shots;
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
+    unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
 };
 
 enum : uint32_t {
@@ -441,6 +442,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// Scalar state the control warp of a CTA group hands to the worker warps
+// before a statevector sweep.
+template <int NW>
+struct CtlState {
+    uint64_t fx[NW], fz[NW];
+    double2 gamma;
+    double log_prob;
+    unsigned long long dust, bytes, moved;
+    uint32_t k, draw, next_noise, ff_pos, ff_end, ro_pos, ro_end, pc;
+    uint32_t cmd;  // 0 = run the sweep at pc, 1 = shot finished
+    uint32_t flags;
+};
+constexpr uint32_t kCtlBytes = 512;
+
 // --------------------------------------------------------------- the shot
 template <typename R, class Grp, int NW>
 struct Shot {
@@ -472,6 +487,7 @@ struct Shot {
     // fused-sweep state (CTA groups only)
     unsigned char* fuse;       // shared scratch: 2 tile buffers, micro-ops, index tables
     bool resolving;            // true while a fused block's opcodes emit micro-ops
+    bool solo;                 // CTA groups: only the control warp is executing
     int n_mops;
     unsigned long long moved;  // statevector bytes actually streamed
 
@@ -492,7 +508,10 @@ struct Shot {
 
     __device__ __forceinline__ void flush_records() {
         if (rec_dirty) {
-            Grp::sync();
+            if (Grp::kCta && solo)
+                __syncwarp();
+            else
+                Grp::sync();
             rec_dirty = false;
         }
     }
@@ -1577,6 +1596,153 @@ struct Shot {
         }
     }
 
+    // Whether instruction pc touches the statevector (needs every thread of a
+    // CTA group) or only scalar state (frame, gamma, records, noise cursor).
+    __device__ __forceinline__ bool needs_all(uint32_t pc) const {
+        const uint4 w0 = __ldg(P.instr + 2 * pc);
+        uint32_t op = w0.x & 0xffu;
+        const uint32_t a1 = w0.y & 0xffffu;
+        if (op >= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED)
+            op -= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED - CLIFFT_OP_MEAS_DORMANT_STATIC;
+        switch (op) {
+            case CLIFFT_OP_ARRAY_CNOT:
+            case CLIFFT_OP_ARRAY_CZ:
+            case CLIFFT_OP_ARRAY_SWAP:
+            case CLIFFT_OP_ARRAY_MULTI_CNOT:
+            case CLIFFT_OP_ARRAY_MULTI_CZ:
+            case CLIFFT_OP_ARRAY_H:
+            case CLIFFT_OP_ARRAY_S:
+            case CLIFFT_OP_ARRAY_S_DAG:
+            case CLIFFT_OP_ARRAY_U4:
+            case CLIFFT_OP_EXPAND:
+            case CLIFFT_OP_EXPAND_T:
+            case CLIFFT_OP_EXPAND_T_DAG:
+            case CLIFFT_OP_EXPAND_ROT:
+            case CLIFFT_OP_MEAS_ACTIVE_DIAGONAL:
+            case CLIFFT_OP_MEAS_ACTIVE_INTERFERE:
+            case CLIFFT_OP_SWAP_MEAS_INTERFERE:
+            case CLIFFT_OP_EXP_VAL: return true;
+            case CLIFFT_OP_ARRAY_T:
+            case CLIFFT_OP_ARRAY_T_DAG:
+            case CLIFFT_OP_ARRAY_ROT:
+            case CLIFFT_OP_ARRAY_U2: return a1 < k;
+            default: return false;
+        }
+    }
+
+    __device__ __forceinline__ CtlState<NW>* ctl() const {
+        return reinterpret_cast<CtlState<NW>*>(reinterpret_cast<unsigned char*>(red) + 3 * 8 * 32 + 64);
+    }
+    __device__ __forceinline__ void publish(uint32_t pc, uint32_t cmd) {
+        if (threadIdx.x == 0) {
+            CtlState<NW>* c = ctl();
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                c->fx[w] = f.x[w];
+                c->fz[w] = f.z[w];
+            }
+            c->gamma = gamma;
+            c->log_prob = log_prob;
+            c->dust = dust;
+            c->bytes = bytes;
+            c->moved = moved;
+            c->k = k;
+            c->draw = draw;
+            c->next_noise = next_noise;
+            c->ff_pos = ff_pos;
+            c->ff_end = ff_end;
+            c->ro_pos = ro_pos;
+            c->ro_end = ro_end;
+            c->pc = pc;
+            c->cmd = cmd;
+            c->flags = (stop ? 1u : 0u) | (discarded ? 2u : 0u) | (reachable ? 4u : 0u);
+        }
+    }
+    __device__ __forceinline__ uint32_t adopt() {
+        const CtlState<NW>* c = ctl();
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            f.x[w] = c->fx[w];
+            f.z[w] = c->fz[w];
+        }
+        gamma = c->gamma;
+        log_prob = c->log_prob;
+        dust = c->dust;
+        bytes = c->bytes;
+        moved = c->moved;
+        k = c->k;
+        draw = c->draw;
+        next_noise = c->next_noise;
+        ff_pos = c->ff_pos;
+        ff_end = c->ff_end;
+        ro_pos = c->ro_pos;
+        ro_end = c->ro_end;
+        stop = (c->flags & 1u) != 0;
+        discarded = (c->flags & 2u) != 0;
+        reachable = (c->flags & 4u) != 0;
+        rec_dirty = false;
+        return c->pc | (c->cmd << 31);
+    }
+    // a statevector step executed by every thread (fused block or one opcode)
+    __device__ __forceinline__ uint32_t run_all(uint32_t pc, bool fuse_on) {
+        uint32_t used = 0;
+        if (fuse_on && k > TileCfg<R>::kBits) used = fused_block(pc);
+        if (!used) {
+            exec(pc);
+            used = 1;
+        }
+        return used;
+    }
+    // CTA groups: warp 0 interprets the bytecode; the other warps join only
+    // for statevector steps, receiving the scalar state through shared memory.
+    __device__ void run_cta(bool fuse_on, bool prof) {
+        const uint32_t n_instr = P.n_instr;
+        if ((threadIdx.x >> 5) == 0) {
+            solo = true;
+            uint32_t pc = 0;
+            while (pc < n_instr && !stop) {
+                const long long c0 = prof ? clock64() : 0;
+                if (needs_all(pc)) {
+                    publish(pc, 0);
+                    __syncthreads();
+                    solo = false;
+                    const uint32_t used = run_all(pc, fuse_on);
+                    solo = true;
+                    __syncthreads();
+                    if (prof) {
+                        const uint32_t op = __ldg(P.instr + 2 * pc).x & 0xffu;
+                        int cat = used > 1 ? 0 : 3;
+                        if ((op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE) ||
+                            (op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL_FORCED &&
+                             op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED))
+                            cat = 1;
+                        else if (op >= CLIFFT_OP_EXPAND && op <= CLIFFT_OP_EXPAND_ROT)
+                            cat = 2;
+                        atomicAdd(K.phase_cycles + cat, (unsigned long long)(clock64() - c0));
+                    }
+                    pc += used;
+                } else {
+                    exec(pc);
+                    if (prof) atomicAdd(K.phase_cycles + 4, (unsigned long long)(clock64() - c0));
+                    ++pc;
+                }
+            }
+            flush_records();
+            publish(0, 1);
+            __syncthreads();
+            solo = false;
+        } else {
+            solo = false;
+            for (;;) {
+                __syncthreads();
+                const uint32_t word = adopt();
+                if (word >> 31) break;
+                run_all(word & 0x7fffffffu, fuse_on);
+                __syncthreads();
+            }
+        }
+    }
+
     // ------------------------------------------------------------ driver
     __device__ __forceinline__ void run(Tally& tally) {
         // SchrodingerState::reset (svm_state.cc:220-267): only v[0] needs a
@@ -1593,6 +1759,7 @@ struct Shot {
         bytes = 0;
         moved = 0;
         resolving = false;
+        solo = false;
         n_mops = 0;
         rec_dirty = false;
         forced = (K.flags & KF_FORCED_MEAS) ? K.forced_meas + shot * P.slots : nullptr;
@@ -1621,16 +1788,14 @@ struct Shot {
 
         const uint32_t n_instr = P.n_instr;
         const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) && fuse != nullptr;
-        for (uint32_t pc = 0; pc < n_instr; ++pc) {
-            if (fuse_on && k > TileCfg<R>::kBits) {
-                const uint32_t used = fused_block(pc);
-                if (used) {
-                    pc += used - 1;
-                    continue;
-                }
+        const bool prof = K.phase_cycles != nullptr && Grp::rank() == 0;
+        if (Grp::kCta) {
+            run_cta(fuse_on, prof);
+        } else {
+            for (uint32_t pc = 0; pc < n_instr; ++pc) {
+                exec(pc);
+                if (stop) break;
             }
-            exec(pc);
-            if (stop) break;
         }
         Grp::sync();
         finish(tally);

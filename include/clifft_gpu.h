@@ -62,6 +62,7 @@ extern "C" {
 #define CLIFFT_GPU_TRACE 0x10u          /* fill meas_prob and the final-state dump */
 #define CLIFFT_GPU_NO_FUSION 0x20u      /* plain executor: one statevector sweep per opcode */
 #define CLIFFT_GPU_FORCE_FUSION 0x40u   /* fuse tile sweeps even when the statevectors fit in L2 */
+#define CLIFFT_GPU_PROFILE 0x80u        /* fill phase_cycles (adds timing atomics; not for benchmarks) */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
 
@@ -115,6 +116,8 @@ typedef struct clifft_gpu_outputs {
     uint32_t group_threads;    /* shot-group size that ran */
     uint32_t state_in_smem;    /* 1 if the statevectors lived in shared memory */
     uint32_t fused;            /* 1 if fused tile sweeps were enabled */
+    uint64_t phase_cycles[5];  /* CLIFFT_GPU_PROFILE: SM cycles in fused blocks, measurements, expansions,
+                                  unfused array sweeps, other opcodes (summed over shot groups) */
 } clifft_gpu_outputs;
 
 /* Upload + validate a program. *out receives an opaque handle. */
