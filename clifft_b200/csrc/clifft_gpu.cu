@@ -704,8 +704,10 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
         if (dev_err != 0) {
             throw ApiError(CLIFFT_GPU_EDEVICE,
-                           dev_err == DEV_ERR_ZERO_NORM ? "active measurement on a zero-norm state"
-                                                        : "device reported an invalid opcode");
+                           dev_err == DEV_ERR_ZERO_NORM  ? "active measurement on a zero-norm state"
+                           : dev_err == DEV_ERR_TIMEOUT  ? "a bounded wait on a bulk-copy barrier timed out"
+                           : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
+                                                           : "unknown device error");
         }
         out->passed_shots = hs[2];
         out->logical_errors = hs[3];

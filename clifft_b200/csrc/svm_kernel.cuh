@@ -1695,51 +1695,46 @@ struct Shot {
     }
     // CTA groups: warp 0 interprets the bytecode; the other warps join only
     // for statevector steps, receiving the scalar state through shared memory.
+    // Every CTA-wide barrier is reached by all warps at the same program point.
     __device__ void run_cta(bool fuse_on, bool prof) {
         const uint32_t n_instr = P.n_instr;
-        if ((threadIdx.x >> 5) == 0) {
-            solo = true;
-            uint32_t pc = 0;
-            while (pc < n_instr && !stop) {
+        const bool ctrl = (threadIdx.x >> 5) == 0;
+        uint32_t pc = 0;
+        for (;;) {
+            if (ctrl) {
+                solo = true;
                 const long long c0 = prof ? clock64() : 0;
-                if (needs_all(pc)) {
-                    publish(pc, 0);
-                    __syncthreads();
-                    solo = false;
-                    const uint32_t used = run_all(pc, fuse_on);
-                    solo = true;
-                    __syncthreads();
-                    if (prof) {
-                        const uint32_t op = __ldg(P.instr + 2 * pc).x & 0xffu;
-                        int cat = used > 1 ? 0 : 3;
-                        if ((op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE) ||
-                            (op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL_FORCED &&
-                             op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED))
-                            cat = 1;
-                        else if (op >= CLIFFT_OP_EXPAND && op <= CLIFFT_OP_EXPAND_ROT)
-                            cat = 2;
-                        atomicAdd(K.phase_cycles + cat, (unsigned long long)(clock64() - c0));
-                    }
-                    pc += used;
-                } else {
+                while (pc < n_instr && !stop && !needs_all(pc)) {
                     exec(pc);
-                    if (prof) atomicAdd(K.phase_cycles + 4, (unsigned long long)(clock64() - c0));
                     ++pc;
                 }
+                flush_records();
+                if (prof) atomicAdd(K.phase_cycles + 4, (unsigned long long)(clock64() - c0));
+                publish(pc, (pc >= n_instr || stop) ? 1u : 0u);
             }
-            flush_records();
-            publish(0, 1);
             __syncthreads();
-            solo = false;
-        } else {
-            solo = false;
-            for (;;) {
-                __syncthreads();
-                const uint32_t word = adopt();
-                if (word >> 31) break;
-                run_all(word & 0x7fffffffu, fuse_on);
-                __syncthreads();
+            uint32_t word;
+            if (ctrl) {
+                word = (pc >= n_instr || stop) ? 0x80000000u : pc;
+            } else {
+                word = adopt();
             }
+            solo = false;
+            if (word >> 31) break;
+            const long long c1 = prof ? clock64() : 0;
+            const uint32_t used = run_all(word, fuse_on);
+            __syncthreads();
+            if (prof) {
+                const uint32_t op = __ldg(P.instr + 2 * word).x & 0xffu;
+                int cat = used > 1 ? 0 : 3;
+                if ((op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE) ||
+                    (op >= CLIFFT_OP_MEAS_ACTIVE_DIAGONAL_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED))
+                    cat = 1;
+                else if (op >= CLIFFT_OP_EXPAND && op <= CLIFFT_OP_EXPAND_ROT)
+                    cat = 2;
+                atomicAdd(K.phase_cycles + cat, (unsigned long long)(clock64() - c1));
+            }
+            pc = word + used;
         }
     }
 
