@@ -89,9 +89,9 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
         profile: bool = False) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
-    records plus everything the call reports. `fusion`: None = automatic (fused
-    tile sweeps when global-memory statevectors outgrow L2), True = always
-    fuse, False = one sweep per opcode (the plain executor)."""
+    records plus everything the call reports. `fusion`: None / True = runs of
+    consecutive opcodes share one pass over a global-memory statevector,
+    False = one pass per opcode (the plain executor)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:

@@ -279,7 +279,8 @@ struct LaunchPlan {
     bool state_in_smem;
     uint64_t state_stride;
     uint32_t nw_words;
-    bool fuse;
+    bool tiles;  // statevector passes stream through the bulk-copy tile engine
+    bool fuse;   // ... and consecutive opcodes fuse into one pass
 };
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
@@ -326,8 +327,8 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
     const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
     auto region_bytes = [&](bool in_smem) {
-        size_t fuse = 0;
-        if (G == 0 && !in_smem && allow_fusion)
+        size_t fuse = 0;  // tile-engine scratch: every CTA group with a global-memory statevector
+        if (G == 0 && !in_smem)
             fuse = precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>() : fuse_smem_bytes<double>();
         return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
                ~size_t(15);
@@ -348,7 +349,8 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         L.regions = 1;
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
-    L.fuse = G == 0 && !L.state_in_smem && allow_fusion;
+    L.tiles = G == 0 && !L.state_in_smem;
+    L.fuse = L.tiles && allow_fusion;
     L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
     CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -569,16 +571,6 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const uint32_t obs_words = (m.num_observables + 31) / 32;
         LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words,
                                    det_words, obs_words, (args->flags & CLIFFT_GPU_NO_FUSION) == 0);
-        if (L.fuse && !(args->flags & CLIFFT_GPU_FORCE_FUSION)) {
-            // Statevectors that stay resident in L2 sweep faster opcode by
-            // opcode; fuse only when the resident set streams from HBM.
-            const size_t amp_b = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
-            const uint64_t resident = uint64_t(L.blocks) * L.regions * L.S * L.state_stride * amp_b;
-            if (resident < (uint64_t(96) << 20))
-                L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words, det_words,
-                                obs_words, false);
-        }
-
         KParams K{};
         K.shots = shots;
         K.first_shot = args->first_shot;
@@ -587,9 +579,9 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
                   (forced_meas ? KF_FORCED_MEAS : 0) | (forced_faults ? KF_FORCED_FAULTS : 0) |
                   (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0) | (L.fuse ? KF_FUSE : 0);
-        K.fuse_bytes = L.fuse ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
-                                                                   : fuse_smem_bytes<double>())
-                              : 0;
+        K.fuse_bytes = L.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
+                                                                    : fuse_smem_bytes<double>())
+                               : 0;
         K.rec_words = rec_words;
         K.det_words = det_words;
         K.obs_words = obs_words;

@@ -577,11 +577,11 @@ struct Shot {
     }
 
     // ---------------------------------------------------------- array ops
-    // Sweeps run in two phases per batch of U items (all loads, then all
-    // stores) so each thread keeps U independent memory requests in flight;
-    // U = 4 for CTA groups streaming large statevectors, 1 for the
-    // shared-memory resident sub-warp groups.
-    static constexpr int U = Grp::kCta ? 4 : 1;
+    // Generic sweeps (shared-memory statevectors, and global ones smaller than
+    // a tile): one item per thread per step. Larger global statevectors stream
+    // through the bulk-copy tile engine instead (stream_tiles), which keeps many
+    // tiles in flight without holding them in registers.
+    static constexpr int U = 1;
 
     template <class V, int UU = U, class Ld, class St>
     __device__ __forceinline__ void sweep(uint64_t n, Ld ld, St st) {
@@ -778,12 +778,40 @@ struct Shot {
             phase_sweep(a, zr, zi);
         }
     }
+    // Statevector passes of a CTA group with a global-memory statevector larger
+    // than one tile go through the bulk-copy tile engine.
+    __device__ __forceinline__ bool tiled(uint32_t kk) const {
+        return Grp::kCta && fuse != nullptr && kk > (uint32_t)TileCfg<R>::kBits;
+    }
+    // one run per tile covering the lowest TILE_BITS axes
+    __device__ __forceinline__ void set_runs_low() {
+        if (Grp::rank() == 0) reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset())[0] = 0;
+    }
+
     // exec_expand / expand_with_phase / exec_expand_{t,t_dag,rot}
     // (svm_kernels.inl:876-1081)
     __device__ __forceinline__ void expand(uint32_t a, bool with_phase, double zr, double zi) {
         const uint64_t half = 1ull << k;
         int x = with_phase ? f.px(a) : 0;
         const T ph = Cx<R>::make(with_phase ? zr : 1.0, with_phase ? (x ? -zi : zi) : 0.0);
+        if (tiled(k)) {
+            if constexpr (Grp::kCta) {
+                constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+                set_runs_low();
+                const int tid = Grp::rank(), nthr = Grp::size();
+                stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, 0, half, 1, [&](T* buf, uint64_t) {
+                    if (with_phase)
+                        for (uint32_t l = tid; l < TN; l += nthr) buf[l] = cmul(buf[l], ph);
+                    __syncthreads();
+                });
+                moved += (2ull << k) * sizeof(T);
+                bytes += (2ull << k) * sizeof(T);
+                k++;
+                scale_magnitude(CGPU_EXPAND_SCALE);
+                if (with_phase && x) phase(make_double2(zr, zi));
+                return;
+            }
+        }
         if (!with_phase) {
             sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i); return p; },
                       [&](const P1& p) { A(half + p.i) = p.x; });
@@ -946,7 +974,25 @@ struct Shot {
         const uint64_t half = 1ull << (k - 1);
         int pxv = f.px(a), pzv = f.pz(a);
         double acc[2] = {0.0, 0.0};
-        {
+        const bool tl = tiled(k);
+        if (tl) {
+            if constexpr (Grp::kCta) {
+                constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+                set_runs_low();
+                const int tid = Grp::rank(), nthr = Grp::size();
+                const uint64_t ntiles = 1ull << (k - MB);
+                stream_tiles(ntiles, ((1ull << k) - 1) & ~(uint64_t)(TN - 1), MB, 0, 0, 0, [&](T* buf, uint64_t t) {
+                    double q = 0.0;
+                    for (uint32_t l = tid; l < TN; l += nthr) q += cnorm_d(buf[l]);
+                    if (t >= ntiles / 2)
+                        acc[1] += q;
+                    else
+                        acc[0] += q;
+                    __syncthreads();
+                });
+                moved += (1ull << k) * sizeof(T);
+            }
+        } else {
             const uint64_t step = (uint64_t)Grp::size();
             for (uint64_t i0 = Grp::rank(); i0 < half; i0 += step * U) {
                 T x[U], y[U];
@@ -965,7 +1011,10 @@ struct Shot {
             }
         }
         group_reduce<Grp, 2>(acc, red);
-        account(1ull << k);
+        if (tl)
+            bytes += (1ull << k) * sizeof(T);
+        else
+            account(1ull << k);
         double p0 = acc[0], p1 = acc[1], total = p0 + p1;
         if (zero_norm(total)) return;
         int want = forced_bit(idx);
@@ -980,10 +1029,20 @@ struct Shot {
         int m_abs = b ^ pxv;
         if (b == 1 && pzv) negate_gamma();
         if (b == 1) {
-            sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i + half); return p; },
-                      [&](const P1& p) { A(p.i) = p.x; });
-            Grp::sync();
-            account(1ull << k);
+            if (tl) {
+                if constexpr (Grp::kCta) {
+                    constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+                    stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, half, 0, 1,
+                                 [&](T*, uint64_t) { __syncthreads(); });
+                    moved += (1ull << k) * sizeof(T);
+                    bytes += (1ull << k) * sizeof(T);
+                }
+            } else {
+                sweep<P1>(half, [&](uint64_t i) { P1 p; p.i = i; p.x = A(i + half); return p; },
+                          [&](const P1& p) { A(p.i) = p.x; });
+                Grp::sync();
+                account(1ull << k);
+            }
         }
         k--;
         double pb = b ? p1 : p0;
@@ -1004,7 +1063,37 @@ struct Shot {
         int pxv = f.px(t), pzv = f.pz(t);
         const uint64_t half = 1ull << t, fb = 1ull << fa;
         double acc[2] = {0.0, 0.0};
-        {
+        // tiled path: the tile spans axes {fa, t} (t is its top local bit);
+        // outputs are the tile positions with the t bit clear
+        const bool tl = tiled(k);
+        uint32_t tr = 0, lf = 0;
+        uint64_t tC = 0;
+        if (tl) {
+            if constexpr (Grp::kCta) {
+                constexpr uint32_t MB = TileCfg<R>::kBits;
+                const uint64_t F = tile_axes((1ull << t) | fb, tr);
+                tC = ((1ull << k) - 1) & ~F;
+                lf = (uint32_t)__popcll(F & (fb - 1));
+                uint64_t* runoff = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
+                if (Grp::rank() < (1 << (MB - tr))) runoff[Grp::rank()] = pdep((uint64_t)Grp::rank() << tr, F);
+                const int tid = Grp::rank(), nthr = Grp::size();
+                const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
+                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, 0, [&](T* buf, uint64_t) {
+                    double qp = 0.0, qm = 0.0;
+                    for (uint32_t l = tid; l < HN; l += nthr) {
+                        uint32_t a0 = swapped ? ((l & ~lfb) | (((l >> lf) & 1u) << lt)) : l;
+                        uint32_t a1 = swapped ? (a0 | lfb) : (l + HN);
+                        T x = buf[a0], y = buf[a1];
+                        qp += cnorm_d(cadd(x, y));
+                        qm += cnorm_d(csub(x, y));
+                    }
+                    acc[0] += qp;
+                    acc[1] += qm;
+                    __syncthreads();
+                });
+                moved += (1ull << k) * sizeof(T);
+            }
+        } else {
             const uint64_t step = (uint64_t)Grp::size();
             for (uint64_t i0 = Grp::rank(); i0 < half; i0 += step * U) {
                 T x[U], y[U];
@@ -1027,7 +1116,10 @@ struct Shot {
             }
         }
         group_reduce<Grp, 2>(acc, red);
-        account((1ull << k) * 2 + (1ull << (k - 1)));
+        if (tl)
+            bytes += ((1ull << k) * 2 + (1ull << (k - 1))) * sizeof(T);
+        else
+            account((1ull << k) * 2 + (1ull << (k - 1)));
         double pp = acc[0], pm = acc[1], total = pp + pm;
         if (zero_norm(total)) return;
         int want = forced_bit(idx);
@@ -1041,7 +1133,35 @@ struct Shot {
         }
         int m_abs = bx ^ pzv;
         const R s = (R)CGPU_INV_SQRT2;
-        if (!swapped) {
+        if (tl) {
+            if constexpr (Grp::kCta) {
+                constexpr uint32_t MB = TileCfg<R>::kBits;
+                const int tid = Grp::rank(), nthr = Grp::size();
+                const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
+                const uint32_t nruns = 1u << (MB - tr);
+                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, nruns / 2, [&](T* buf, uint64_t) {
+                    if (!swapped) {
+                        for (uint32_t l = tid; l < HN; l += nthr) {
+                            T x = buf[l], y = buf[l + HN];
+                            buf[l] = cscale(bx ? csub(x, y) : cadd(x, y), s);
+                        }
+                        __syncthreads();
+                    } else {
+                        // outputs with the fa bit clear read positions the fa-set outputs overwrite
+                        for (int pass = 0; pass < 2; ++pass) {
+                            for (uint32_t j = tid; j < HN / 2; j += nthr) {
+                                uint32_t l = (uint32_t)ins0(j, lf) | (pass ? lfb : 0u);
+                                uint32_t a0 = pass ? ((l & ~lfb) | HN) : l;
+                                T x = buf[a0], y = buf[a0 | lfb];
+                                buf[l] = cscale(bx ? csub(x, y) : cadd(x, y), s);
+                            }
+                            __syncthreads();
+                        }
+                    }
+                });
+                moved += (1ull << k) * sizeof(T) + (1ull << (k - 1)) * sizeof(T);
+            }
+        } else if (!swapped) {
             sweep<P2>(half, [&](uint64_t i) { P2 p; p.i = i; p.x = A(i); p.y = A(i + half); return p; },
                       [&](const P2& p) { A(p.i) = cscale(bx ? csub(p.x, p.y) : cadd(p.x, p.y), s); });
             Grp::sync();
@@ -1422,7 +1542,7 @@ struct Shot {
     // Fused tile sweep starting at `pc` (CTA groups, statevector in global
     // memory, k > tile bits). Returns the number of instructions consumed, 0
     // when the opcode at `pc` cannot start a block.
-    __device__ uint32_t fused_block(uint32_t pc) {
+    __device__ uint32_t fused_block(uint32_t pc, int max_ops) {
         constexpr uint32_t MB = TileCfg<R>::kBits;
         uint64_t uni = 0;
         int nsweep = 0;
@@ -1458,7 +1578,7 @@ struct Shot {
             if (m) {
                 const uint64_t cand = uni | m;
                 uint32_t rr;
-                if ((uint32_t)__popcll(cand) >= MB || nsweep >= kMaxMicroOps) break;
+                if ((uint32_t)__popcll(cand) >= MB || nsweep >= max_ops) break;
                 tile_axes(cand, rr);
                 if (MB - rr > (uint32_t)kMaxRunsLog2) break;
                 uni = cand;
@@ -1686,7 +1806,7 @@ struct Shot {
     // a statevector step executed by every thread (fused block or one opcode)
     __device__ __forceinline__ uint32_t run_all(uint32_t pc, bool fuse_on) {
         uint32_t used = 0;
-        if (fuse_on && k > TileCfg<R>::kBits) used = fused_block(pc);
+        if (tiled(k)) used = fused_block(pc, fuse_on ? kMaxMicroOps : 1);
         if (!used) {
             exec(pc);
             used = 1;
@@ -1782,7 +1902,7 @@ struct Shot {
         Grp::sync();
 
         const uint32_t n_instr = P.n_instr;
-        const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) && fuse != nullptr;
+        const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) != 0;
         const bool prof = K.phase_cycles != nullptr && Grp::rank() == 0;
         if (Grp::kCta) {
             run_cta(fuse_on, prof);

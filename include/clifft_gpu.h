@@ -60,8 +60,8 @@ extern "C" {
 #define CLIFFT_GPU_FORCED_FAULTS 0x04u  /* fault sites / channels / readout flips from the CSR inputs */
 #define CLIFFT_GPU_DEVICE_PTRS 0x08u    /* every input/output pointer is a device pointer */
 #define CLIFFT_GPU_TRACE 0x10u          /* fill meas_prob and the final-state dump */
-#define CLIFFT_GPU_NO_FUSION 0x20u      /* plain executor: one statevector sweep per opcode */
-#define CLIFFT_GPU_FORCE_FUSION 0x40u   /* fuse tile sweeps even when the statevectors fit in L2 */
+#define CLIFFT_GPU_NO_FUSION 0x20u      /* plain executor: one statevector pass per opcode */
+#define CLIFFT_GPU_FORCE_FUSION 0x40u   /* reserved (fusion is on unless CLIFFT_GPU_NO_FUSION) */
 #define CLIFFT_GPU_PROFILE 0x80u        /* fill phase_cycles (adds timing atomics; not for benchmarks) */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
