@@ -595,10 +595,11 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
             K.state_global = buf.alloc(size_t(L.blocks) * L.regions * L.S * L.state_stride * amp);
         const size_t n_counters = 5 + m.num_observables;
         const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;
-        const size_t scratch_words = 2 + n_counters + (profile ? 8 : 0);
+        const size_t scratch_words = 2 + n_counters + (profile ? 8 : 0) + 8;
         auto* scratch = static_cast<unsigned long long*>(buf.alloc(scratch_words * 8 + 64));
         CUDA_OK(cudaMemsetAsync(scratch, 0, scratch_words * 8 + 64, st));
         K.phase_cycles = profile ? scratch + 2 + n_counters : nullptr;
+        K.error_info = scratch + scratch_words - 8;
         K.work_counter = scratch;
         K.error_word = reinterpret_cast<int*>(scratch + 1);
         K.counters = scratch + 2;
@@ -695,11 +696,17 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
             for (uint32_t w = 0; w < nwo; ++w) out->final_pz[s * nwo + w] = hpz[s * nwt + w];
         const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
         if (dev_err != 0) {
-            throw ApiError(CLIFFT_GPU_EDEVICE,
-                           dev_err == DEV_ERR_ZERO_NORM  ? "active measurement on a zero-norm state"
-                           : dev_err == DEV_ERR_TIMEOUT  ? "a bounded wait on a bulk-copy barrier timed out"
-                           : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
-                                                           : "unknown device error");
+            std::string msg = dev_err == DEV_ERR_ZERO_NORM    ? "active measurement on a zero-norm state"
+                              : dev_err == DEV_ERR_TIMEOUT    ? "a bounded wait on a bulk-copy barrier timed out"
+                              : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
+                                                              : "unknown device error";
+            if (dev_err == DEV_ERR_TIMEOUT) {
+                const unsigned long long* e = hs.data() + scratch_words - 8;
+                msg += " (pass " + std::to_string(e[0]) + ", instruction " + std::to_string(e[1]) + ", tile " +
+                       std::to_string(e[2]) + "/" + std::to_string(e[3]) + ", run log2 " + std::to_string(e[4]) +
+                       ", k " + std::to_string(e[5]) + ")";
+            }
+            throw ApiError(CLIFFT_GPU_EDEVICE, msg);
         }
         out->passed_shots = hs[2];
         out->logical_errors = hs[3];

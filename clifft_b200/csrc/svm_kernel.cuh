@@ -99,6 +99,7 @@ struct KParams {
     unsigned long long* work_counter;
     unsigned long long* counters;  // [0] passed, [1] logical errors, [2] dust clamps, [3] algorithmic bytes, [4] streamed bytes, [5..] observable ones
     int* error_word;               // first device-side error code (0 = none)
+    unsigned long long* error_info;  // where a bounded wait gave up: site, pc, tile, tiles, r, k
     // forced inputs
     const uint8_t* forced_meas;
     const uint32_t* fault_off;
@@ -799,6 +800,7 @@ struct Shot {
                 constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
                 set_runs_low();
                 const int tid = Grp::rank(), nthr = Grp::size();
+                cur_site = 1;
                 stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, 0, half, 1, [&](T* buf, uint64_t) {
                     if (with_phase)
                         for (uint32_t l = tid; l < TN; l += nthr) buf[l] = cmul(buf[l], ph);
@@ -981,6 +983,7 @@ struct Shot {
                 set_runs_low();
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint64_t ntiles = 1ull << (k - MB);
+                cur_site = 2;
                 stream_tiles(ntiles, ((1ull << k) - 1) & ~(uint64_t)(TN - 1), MB, 0, 0, 0, [&](T* buf, uint64_t t) {
                     double q = 0.0;
                     for (uint32_t l = tid; l < TN; l += nthr) q += cnorm_d(buf[l]);
@@ -1032,6 +1035,7 @@ struct Shot {
             if (tl) {
                 if constexpr (Grp::kCta) {
                     constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+                    cur_site = 3;
                     stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, half, 0, 1,
                                  [&](T*, uint64_t) { __syncthreads(); });
                     moved += (1ull << k) * sizeof(T);
@@ -1078,6 +1082,7 @@ struct Shot {
                 if (Grp::rank() < (1 << (MB - tr))) runoff[Grp::rank()] = pdep((uint64_t)Grp::rank() << tr, F);
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
+                cur_site = 4;
                 stream_tiles(1ull << (k - MB), tC, tr, 0, 0, 0, [&](T* buf, uint64_t) {
                     double qp = 0.0, qm = 0.0;
                     for (uint32_t l = tid; l < HN; l += nthr) {
@@ -1139,6 +1144,7 @@ struct Shot {
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
                 const uint32_t nruns = 1u << (MB - tr);
+                cur_site = 5;
                 stream_tiles(1ull << (k - MB), tC, tr, 0, 0, nruns / 2, [&](T* buf, uint64_t) {
                     if (!swapped) {
                         for (uint32_t l = tid; l < HN; l += nthr) {
@@ -1340,6 +1346,7 @@ struct Shot {
     // Executes instruction `pc` (the dispatch of execute_internal,
     // svm_kernels.inl:2183-2646; forced opcodes share the sampling handlers).
     __device__ __forceinline__ void exec(uint32_t pc) {
+        cur_pc = pc;
         const uint4* ip = P.instr;
         const uint4 w0 = __ldg(ip + 2 * pc);
         uint32_t op = w0.x & 0xffu;
@@ -1464,6 +1471,8 @@ struct Shot {
     // tile) go to v[store_add + ...]. Bulk copies (TMA) run kStages tiles
     // ahead; `compute(buf, t)` is called by every thread and must synchronise
     // the CTA before it returns. Returns false after a barrier timeout.
+    uint32_t cur_pc = 0;   // instruction being executed (diagnostics)
+    uint32_t cur_site = 0; // which statevector pass is streaming (diagnostics)
     template <class Compute>
     __device__ bool stream_tiles(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add, uint64_t store_add,
                                  uint32_t store_runs, Compute compute) {
@@ -1523,7 +1532,14 @@ struct Shot {
         }
         if (!ok_all) {
             // drain (bounded) every load still in flight before the buffers go away
-            if (tid == 0) atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT);
+            if (tid == 0 && atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT) == 0 && K.error_info) {
+                K.error_info[0] = cur_site;
+                K.error_info[1] = cur_pc;
+                K.error_info[2] = t;
+                K.error_info[3] = ntiles;
+                K.error_info[4] = r;
+                K.error_info[5] = k;
+            }
             for (uint64_t q = t; q < ntiles && q < t + kStages - 1; ++q) {
                 const uint32_t st = (uint32_t)(q % kStages);
                 for (uint32_t it = 0; it < (1u << 20); ++it)
@@ -1607,6 +1623,7 @@ struct Shot {
         const MicroOp* mops = reinterpret_cast<const MicroOp*>(fuse + fuse_mops_offset());
         const int tid = Grp::rank(), nthr = Grp::size();
         const int nm = n_mops;
+        cur_site = 6;
         stream_tiles(1ull << (k - MB), C, r, 0, 0, 1u << (MB - r), [&](T* buf, uint64_t) {
             for (int j = 0; j < nm; ++j) {
                 apply_micro(mops[j], buf, tid, nthr);
