@@ -704,7 +704,8 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
                 const unsigned long long* e = hs.data() + scratch_words - 8;
                 msg += " (pass " + std::to_string(e[0]) + ", instruction " + std::to_string(e[1]) + ", tile " +
                        std::to_string(e[2]) + "/" + std::to_string(e[3]) + ", run log2 " + std::to_string(e[4]) +
-                       ", k " + std::to_string(e[5]) + ")";
+                       ", k " + std::to_string(e[5]) + ", barrier word " + std::to_string(e[6]) +
+                       ", waited " + std::to_string(e[7]) + " cycles)";
             }
             throw ApiError(CLIFFT_GPU_EDEVICE, msg);
         }

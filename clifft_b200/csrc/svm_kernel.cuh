@@ -487,14 +487,16 @@ struct Shot {
     double* meas_prob;
     // fused-sweep state (CTA groups only)
     unsigned char* fuse;       // shared scratch: 2 tile buffers, micro-ops, index tables
+    uint32_t* bar_phase;       // CTA groups: bit st = parity of the phase stage st's barrier is in;
+                               // bit 31 set once a wait timed out (the barriers are then unusable)
     bool resolving;            // true while a fused block's opcodes emit micro-ops
     bool solo;                 // CTA groups: only the control warp is executing
     int n_mops;
     unsigned long long moved;  // statevector bytes actually streamed
 
     __device__ __forceinline__ Shot(const DevProg& p, const KParams& kp, T* vv, uint32_t* r, uint32_t* d,
-                                    uint32_t* o, double* rd, unsigned char* fz, uint64_t s)
-        : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s), fuse(fz) {}
+                                    uint32_t* o, double* rd, unsigned char* fz, uint32_t* bp, uint64_t s)
+        : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s), fuse(fz), bar_phase(bp) {}
 
     __device__ __forceinline__ T& A(uint64_t i) { return v[i * S]; }
     // algorithmic bytes of an opcode (per-opcode definition); streamed bytes
@@ -1484,12 +1486,16 @@ struct Shot {
         const uint32_t nruns = 1u << (MB - r);
         const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
         const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+        // The stage barriers are initialised once per CTA (kernel entry); each
+        // call continues from the phase every stage is in, tracked in
+        // *bar_phase identically by every thread.
+        uint32_t phase = *bar_phase;
+        if (phase >> 31) {
+            stop = true;
+            return false;
+        }
         // statevector writes made by ordinary stores must be visible to the copy engine
         fence_async_global();
-        if (tid == 0) {
-            for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
-            mbar_fence_init();
-        }
         __syncthreads();
         auto issue_load = [&](uint64_t t) {
             const uint32_t st = (uint32_t)(t % kStages);
@@ -1502,16 +1508,20 @@ struct Shot {
         if (warp == 0)
             for (uint64_t t = 0; t < ntiles && t < (uint64_t)(kStages - 1); ++t) issue_load(t);
         bool ok_all = true;
+        long long waited = 0;
         uint64_t t = 0;
         for (; t < ntiles; ++t) {
             const uint32_t st = (uint32_t)(t % kStages);
-            const uint32_t parity = (uint32_t)((t / kStages) & 1u);
+            const uint32_t parity = (phase >> st) & 1u;
             uint32_t ok = 0;
+            const long long w0 = clock64();
             for (uint32_t it = 0; it < (1u << 20) && !ok; ++it) ok = mbar_try_wait(&bars[st], parity);
+            waited = clock64() - w0;
             if (__syncthreads_or(!ok)) {
                 ok_all = false;
                 break;
             }
+            phase ^= 1u << st;
             T* buf = bufs + st * TN;
             compute(buf, t);
             if (store_runs) {
@@ -1539,18 +1549,23 @@ struct Shot {
                 K.error_info[3] = ntiles;
                 K.error_info[4] = r;
                 K.error_info[5] = k;
+                K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[t % kStages]);
+                K.error_info[7] = (unsigned long long)waited;
             }
             for (uint64_t q = t; q < ntiles && q < t + kStages - 1; ++q) {
                 const uint32_t st = (uint32_t)(q % kStages);
                 for (uint32_t it = 0; it < (1u << 20); ++it)
-                    if (mbar_try_wait(&bars[st], (uint32_t)((q / kStages) & 1u))) break;
+                    if (mbar_try_wait(&bars[st], (phase >> st) & 1u)) break;
+                phase ^= 1u << st;
             }
+            phase |= 1u << 31;
             stop = true;
         }
         if (warp == 0) {
             bulk_wait_all();
             fence_async_global();
         }
+        *bar_phase = phase;
         __syncthreads();
         return ok_all;
     }
@@ -2040,6 +2055,17 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
     uint32_t* det = rec + (size_t)K.rec_words * S;
     uint32_t* obs = det + (size_t)K.det_words * S;
     unsigned char* fz = K.fuse_bytes ? rbase + state_bytes + rec_bytes : nullptr;
+    uint32_t bar_phase = 0;
+    if (Grp::kCta && fz != nullptr) {
+        // tile-engine stage barriers: initialised once, reused by every pass
+        // of every shot this CTA runs
+        if (threadIdx.x == 0) {
+            uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW>::fuse_bar_offset());
+            for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+    }
     T* v;
     if (K.state_in_smem) {
         v = reinterpret_cast<T*>(rbase) + Grp::slot();
@@ -2051,7 +2077,8 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
     for (;;) {
         unsigned long long base = 0;
         if (Grp::kCta) {
-            if (threadIdx.x == 0) *bcast = atomicAdd(K.work_counter, 1ull);
+            if (threadIdx.x == 0)
+                *bcast = (bar_phase >> 31) ? ~0ull : atomicAdd(K.work_counter, 1ull);
             __syncthreads();
             base = *bcast;
             __syncthreads();
@@ -2062,7 +2089,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
         if (base >= K.shots) break;
         const unsigned long long shot = base + Grp::slot();
         if (shot < K.shots) {
-            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, fz, shot);
+            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, fz, &bar_phase, shot);
             s.run(tally);
         }
         if (!Grp::kCta) __syncwarp();
