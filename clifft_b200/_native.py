@@ -79,6 +79,8 @@ def lib():
             L.clifft_gpu_free.argtypes = [P]
             L.clifft_gpu_sample.restype = ctypes.c_int
             L.clifft_gpu_sample.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.POINTER(Outputs)]
+            L.clifft_gpu_sample_noalloc.restype = ctypes.c_int
+            L.clifft_gpu_sample_noalloc.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.POINTER(Outputs)]
             L.clifft_gpu_backend_name.restype = ctypes.c_char_p
             L.clifft_gpu_last_error.restype = ctypes.c_char_p
             L.clifft_gpu_program_peak_rank.restype = ctypes.c_uint32
@@ -92,7 +94,9 @@ def lib():
 EXPORTED_SYMBOLS = (
     "clifft_gpu_load", "clifft_gpu_free", "clifft_gpu_sample", "clifft_gpu_backend_name",
     "clifft_gpu_last_error", "clifft_gpu_program_peak_rank", "clifft_gpu_program_device_bytes",
+    "clifft_gpu_sample_noalloc",
 )
+NOALLOC_SCRATCH_WORDS = 512  # CLIFFT_GPU_NOALLOC_SCRATCH_WORDS
 
 
 def check(rc: int, what: str) -> None:

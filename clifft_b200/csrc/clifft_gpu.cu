@@ -726,3 +726,152 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ allocation-free sampling
+// clifft_gpu_sample_noalloc keeps its launch scratch (work counter, error
+// word, counters, timeout diagnostics) in this module's own device array
+// instead of stream-ordered allocations. One array exists per device per
+// process, so calls that overlap on one device race on it.
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[CLIFFT_GPU_NOALLOC_SCRATCH_WORDS];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Address of g_noalloc_scratch on `dev` (which must be current), looked up
+// once per device.
+unsigned long long* noalloc_scratch(int dev) {
+    if (dev < 0 || dev >= kNoallocMaxDevices) invalid("device ordinal out of range for the static scratch table");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_OK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
+                              clifft_gpu_outputs* out) {
+    return guarded([&] {
+        if (!prog || !args || !out) invalid("null argument");
+        const clifft_program_image& m = prog->meta;
+        const uint64_t shots = args->shots;
+        if (args->precision != CLIFFT_GPU_FP32 && args->precision != CLIFFT_GPU_FP64)
+            invalid("precision must be CLIFFT_GPU_FP32 or CLIFFT_GPU_FP64");
+        const uint32_t gt = args->group_threads;
+        if (gt != 0 && !(gt <= 32 && (gt & (gt - 1)) == 0) && (gt % 32 != 0 || gt > 1024))
+            invalid("group_threads must be 0, a power of two up to 32, or a multiple of 32 up to 1024");
+        if (!(args->flags & CLIFFT_GPU_DEVICE_PTRS))
+            invalid("clifft_gpu_sample_noalloc needs CLIFFT_GPU_DEVICE_PTRS: every input and output "
+                    "buffer must already be in device memory");
+        if (args->flags & (CLIFFT_GPU_TRACE | CLIFFT_GPU_PROFILE))
+            invalid("clifft_gpu_sample_noalloc does not support CLIFFT_GPU_TRACE or CLIFFT_GPU_PROFILE");
+        const bool forced_meas = (args->flags & CLIFFT_GPU_FORCED_MEAS) != 0;
+        const bool forced_faults = (args->flags & CLIFFT_GPU_FORCED_FAULTS) != 0;
+        if (forced_meas && !args->forced_meas && m.total_meas_slots > 0)
+            invalid("CLIFFT_GPU_FORCED_MEAS needs forced_meas");
+        if (forced_faults && (!args->fault_offsets || !args->readout_offsets))
+            invalid("CLIFFT_GPU_FORCED_FAULTS needs fault_offsets and readout_offsets");
+        // scratch layout: work counter, error word, 5 totals, one counter per
+        // observable, 8 words of timeout diagnostics
+        const size_t n_counters = 5 + size_t(m.num_observables);
+        const size_t words = 2 + n_counters + 8;
+        if (words > CLIFFT_GPU_NOALLOC_SCRATCH_WORDS)
+            invalid("clifft_gpu_sample_noalloc: a program with " + std::to_string(m.num_observables) +
+                    " observables needs " + std::to_string(words) + " scratch words; the static scratch holds " +
+                    std::to_string(CLIFFT_GPU_NOALLOC_SCRATCH_WORDS) + " (at most " +
+                    std::to_string(CLIFFT_GPU_NOALLOC_SCRATCH_WORDS - 15) + " observables)");
+        out->passed_shots = 0;
+        out->logical_errors = 0;
+        out->dust_clamps = 0;
+        out->algorithmic_bytes = 0;
+        out->streamed_bytes = 0;
+        out->kernel_launches = 0;
+        out->kernel_ms = 0.f;
+        if (shots == 0) return;
+        CUDA_OK(cudaSetDevice(prog->device));
+        unsigned long long* scratch = noalloc_scratch(prog->device);
+        cudaStream_t st = static_cast<cudaStream_t>(args->stream);
+
+        const uint32_t rec_words = (m.total_meas_slots + 31) / 32;
+        const uint32_t det_words = (m.num_detectors + 31) / 32;
+        const uint32_t obs_words = (m.num_observables + 31) / 32;
+        LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words, det_words,
+                                   obs_words, (args->flags & CLIFFT_GPU_NO_FUSION) == 0);
+        if (!L.state_in_smem)
+            invalid("clifft_gpu_sample_noalloc: the statevectors of this program (peak rank " +
+                    std::to_string(m.peak_rank) +
+                    ") do not fit in shared memory with this launch shape, and this entry point has no "
+                    "global-memory statevector slab; use clifft_gpu_sample");
+        KParams K{};
+        K.shots = shots;
+        K.first_shot = args->first_shot;
+        K.seed = args->seed;
+        K.dust_eps = args->dust_eps > 0.0 ? args->dust_eps : (args->precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
+        K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) | (forced_meas ? KF_FORCED_MEAS : 0) |
+                  (forced_faults ? KF_FORCED_FAULTS : 0);
+        K.fuse_bytes = 0;
+        K.rec_words = rec_words;
+        K.det_words = det_words;
+        K.obs_words = obs_words;
+        K.meas_out_words = (m.num_measurements + 63) / 64;
+        K.det_out_words = (m.num_detectors + 63) / 64;
+        K.obs_out_words = (m.num_observables + 63) / 64;
+        K.state_in_smem = 1;
+        K.state_stride = L.state_stride;
+        K.state_global = nullptr;
+        // every scratch word the kernel reads must start at zero: cleared on the
+        // call's stream ahead of the launch
+        CUDA_OK(cudaMemsetAsync(scratch, 0, words * 8, st));
+        K.phase_cycles = nullptr;
+        K.work_counter = scratch;
+        K.error_word = reinterpret_cast<int*>(scratch + 1);
+        K.counters = scratch + 2;
+        K.error_info = scratch + words - 8;
+        K.forced_meas = forced_meas ? args->forced_meas : nullptr;
+        if (forced_faults) {
+            K.fault_off = args->fault_offsets;
+            K.ro_off = args->readout_offsets;
+            K.fault_sites = args->fault_sites;
+            K.fault_chan = args->fault_channels;
+            K.ro_entries = args->readout_entries;
+        }
+        K.out_meas = K.meas_out_words ? out->meas : nullptr;
+        K.out_det = K.det_out_words ? out->det : nullptr;
+        K.out_obs = K.obs_out_words ? out->obs : nullptr;
+        K.out_exp = m.num_exp_vals ? out->exp_vals : nullptr;
+        K.out_survived = out->survived;
+
+        L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
+        CUDA_OK(cudaGetLastError());
+        unsigned long long hs[CLIFFT_GPU_NOALLOC_SCRATCH_WORDS];
+        CUDA_OK(cudaMemcpyAsync(hs, scratch, words * 8, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
+        if (dev_err != 0)
+            throw ApiError(CLIFFT_GPU_EDEVICE, dev_err == DEV_ERR_ZERO_NORM    ? "active measurement on a zero-norm state"
+                                               : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
+                                                                               : "unknown device error");
+        out->passed_shots = hs[2];
+        out->logical_errors = hs[3];
+        out->dust_clamps = hs[4];
+        out->algorithmic_bytes = hs[5];
+        out->streamed_bytes = hs[6];
+        if (out->observable_ones)
+            for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[7 + i];
+        out->kernel_launches = 1;
+        out->group_threads = L.G ? uint32_t(L.G) : uint32_t(L.threads);
+        out->state_in_smem = 1;
+        out->fused = 0;
+        for (int i = 0; i < 5; ++i) out->phase_cycles[i] = 0;
+    });
+}
+
+}  // extern "C"

@@ -131,6 +131,42 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
 const char* clifft_gpu_backend_name(void);
 /* Message of the last failing call on this host thread. */
 const char* clifft_gpu_last_error(void);
+/*
+ * clifft_gpu_sample_noalloc -- clifft_gpu_sample without any device memory
+ * allocation. No counterpart in the reference (its CPU executor allocates
+ * per call); this entry point exists for callers that cannot allocate device
+ * memory while they sample: a process whose free device memory is owned by
+ * another allocator (a framework's caching allocator that reserved it), or a
+ * decoding loop with a fixed device-memory budget in which an allocation that
+ * fails mid-run is not acceptable.
+ *
+ * It runs the same kernel as clifft_gpu_sample and returns the same records
+ * and counters for the same arguments. Differences and limits:
+ *  - CLIFFT_GPU_DEVICE_PTRS is required: every input and output buffer is a
+ *    device buffer the caller owns. CLIFFT_GPU_TRACE and CLIFFT_GPU_PROFILE
+ *    are rejected. kernel_ms is not measured (0).
+ *  - The program's statevectors must fit in shared memory with the chosen
+ *    launch shape (there is no global-memory statevector slab); otherwise the
+ *    call returns CLIFFT_GPU_EINVAL and clifft_gpu_sample must be used.
+ *  - Launch scratch lives in a file-scope device array of
+ *    CLIFFT_GPU_NOALLOC_SCRATCH_WORDS 64-bit words (4 KiB) per device: work
+ *    counter, error word, 5 totals, one counter per observable and 8 words of
+ *    diagnostics, so a program may have at most
+ *    CLIFFT_GPU_NOALLOC_SCRATCH_WORDS - 15 observables; larger programs get
+ *    CLIFFT_GPU_EINVAL. Those words must start at zero: the call clears them
+ *    itself on args->stream before its launch, so nothing needs to be zeroed
+ *    beforehand.
+ *  - There is one such array per device per process. Calls that overlap on
+ *    the same device (other streams or other host threads) race on it and
+ *    their results are undefined: serialise them. The call synchronises its
+ *    stream before it returns.
+ *  - The first call on each device looks up the array's device address with
+ *    that device current (cudaGetSymbolAddress); make that first call before
+ *    any stream capture begins on that device.
+ */
+#define CLIFFT_GPU_NOALLOC_SCRATCH_WORDS 512u
+int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
+                              clifft_gpu_outputs* out);
 /* Program metadata accessors (host memory). */
 uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog);
 uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog);
