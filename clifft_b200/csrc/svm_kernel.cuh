@@ -578,6 +578,62 @@ struct Shot {
         Frame<NW>::put(f.z, a, zb);
         Frame<NW>::put(f.z, b, za);
     }
+    // A run of frame opcodes (FRAME_CNOT / CZ / H / S / S_DAG / SWAP: most of
+    // a compiled Clifford circuit) executed with the frame and gamma in
+    // registers and the next instruction word fetched one step ahead. The
+    // updates and their order are those of the per-opcode handlers above.
+    // Returns the first pc at or after `pc` that is not a frame opcode.
+    __device__ __forceinline__ uint32_t frame_run(uint32_t pc, uint32_t n_instr) {
+        if (pc >= n_instr) return pc;
+        uint4 w = __ldg(P.instr + 2 * pc);
+        if ((w.x & 0xffu) > CLIFFT_OP_FRAME_SWAP) return pc;
+        Frame<NW> ff = f;
+        double2 g = gamma;
+        for (;;) {
+            const uint32_t op = w.x & 0xffu;
+            if (op > CLIFFT_OP_FRAME_SWAP) break;
+            const uint32_t a = w.y & 0xffffu, b = w.y >> 16;
+            const uint4 nxt = pc + 1 < n_instr ? __ldg(P.instr + 2 * (pc + 1)) : make_uint4(0xffu, 0u, 0u, 0u);
+            const int xa = ff.px(a), xb = ff.px(b);
+            switch (op) {
+                case CLIFFT_OP_FRAME_CNOT:
+                    Frame<NW>::flip(ff.x, b, xa);
+                    Frame<NW>::flip(ff.z, a, ff.pz(b));
+                    break;
+                case CLIFFT_OP_FRAME_CZ:
+                    if (xa & xb) g = make_double2(-g.x, -g.y);
+                    Frame<NW>::flip(ff.z, b, xa);
+                    Frame<NW>::flip(ff.z, a, xb);
+                    break;
+                case CLIFFT_OP_FRAME_H: {
+                    const int za = ff.pz(a);
+                    if (xa & za) g = make_double2(-g.x, -g.y);
+                    Frame<NW>::put(ff.x, a, za);
+                    Frame<NW>::put(ff.z, a, xa);
+                    break;
+                }
+                case CLIFFT_OP_FRAME_S:
+                case CLIFFT_OP_FRAME_S_DAG:
+                    if (xa) g = dmul(g, make_double2(0.0, op == CLIFFT_OP_FRAME_S_DAG ? -1.0 : 1.0));
+                    Frame<NW>::flip(ff.z, a, xa);
+                    break;
+                default: {  // FRAME_SWAP
+                    const int za = ff.pz(a), zb = ff.pz(b);
+                    Frame<NW>::put(ff.x, a, xb);
+                    Frame<NW>::put(ff.x, b, xa);
+                    Frame<NW>::put(ff.z, a, zb);
+                    Frame<NW>::put(ff.z, b, za);
+                    break;
+                }
+            }
+            ++pc;
+            w = nxt;
+            if (pc >= n_instr) break;
+        }
+        f = ff;
+        gamma = g;
+        return pc;
+    }
 
     // ---------------------------------------------------------- array ops
     // Generic sweeps (shared-memory statevectors, and global ones smaller than
@@ -1856,7 +1912,9 @@ struct Shot {
             if (ctrl) {
                 solo = true;
                 const long long c0 = prof ? clock64() : 0;
-                while (pc < n_instr && !stop && !needs_all(pc)) {
+                while (pc < n_instr && !stop) {
+                    pc = frame_run(pc, n_instr);
+                    if (pc >= n_instr || needs_all(pc)) break;
                     exec(pc);
                     ++pc;
                 }
@@ -1940,6 +1998,8 @@ struct Shot {
             run_cta(fuse_on, prof);
         } else {
             for (uint32_t pc = 0; pc < n_instr; ++pc) {
+                pc = frame_run(pc, n_instr);
+                if (pc >= n_instr) break;
                 exec(pc);
                 if (stop) break;
             }
