@@ -87,11 +87,13 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
-        profile: bool = False) -> Dict[str, object]:
+        profile: bool = False, autotune: bool = True) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None / True = runs of
     consecutive opcodes share one pass over a global-memory statevector,
-    False = one pass per opcode (the plain executor)."""
+    False = one pass per opcode (the plain executor). `autotune`: with
+    group_threads == 0, let the library time candidate launch shapes on the
+    first large call and keep the fastest (False = fixed heuristic)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:
@@ -126,6 +128,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_TRACE
     if profile:
         flags |= N.CLIFFT_GPU_PROFILE
+    if not autotune:
+        flags |= N.CLIFFT_GPU_NO_AUTOTUNE
     if fusion is False:
         flags |= N.CLIFFT_GPU_NO_FUSION
     elif fusion is True:

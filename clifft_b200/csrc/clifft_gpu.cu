@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -247,6 +248,9 @@ struct clifft_gpu_program {
     size_t blob_bytes = 0;
     std::vector<uint8_t> expected_host;
     int device = 0;
+    // launch shapes picked by the autotuner, per (precision, mode) key
+    std::mutex tune_mu;
+    std::map<uint32_t, uint32_t> tuned;
 };
 
 namespace {
@@ -317,7 +321,7 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     else if (group_req > 32)
         G = 0;
     else
-        G = (state_bytes <= 16384) ? default_group(p.meta.peak_rank) : 0;
+        G = (state_bytes <= 16384) ? default_group(p.meta.peak_rank) : (state_bytes <= (size_t(1) << 20) ? 32 : 0);
     if (G != 0 && (G & (G - 1))) invalid("group_threads below 32 must be a power of two");
     L.G = G;
     L.S = G ? 32 / G : 1;
@@ -374,6 +378,26 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     L.state_stride = stride;
     return L;
 }
+
+// Launch shapes the autotuner tries (group_threads encoding): sub-warp groups
+// around the heuristic width for shared-memory statevectors, warp or CTA
+// groups for L2/HBM-resident ones up to 4 MiB. Larger statevectors have one
+// sensible shape (a CTA streaming tiles) and are not tuned.
+std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t precision) {
+    const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
+    const size_t state_bytes = (size_t(1) << p.meta.peak_rank) * amp;
+    std::vector<uint32_t> c;
+    if (state_bytes <= 16384) {
+        const int g = default_group(p.meta.peak_rank);
+        for (int x : {g / 2, g, g * 2})
+            if (x >= 1 && x <= 32) c.push_back(uint32_t(x));
+    } else if (state_bytes <= (size_t(4) << 20)) {
+        c = {32, 16, 256, 512};
+    }
+    return c;
+}
+
+constexpr uint64_t kTuneMinShots = 1024;
 
 }  // namespace
 
@@ -569,8 +593,23 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         const uint32_t rec_words = (m.total_meas_slots + 31) / 32;
         const uint32_t det_words = (m.num_detectors + 31) / 32;
         const uint32_t obs_words = (m.num_observables + 31) / 32;
-        LaunchPlan L = plan_launch(*prog, args->precision, args->group_threads, shots, rec_words,
-                                   det_words, obs_words, (args->flags & CLIFFT_GPU_NO_FUSION) == 0);
+        const bool allow_fusion = (args->flags & CLIFFT_GPU_NO_FUSION) == 0;
+        // autotuned launch shape (group_threads == 0)
+        const uint32_t tune_key = args->precision | (allow_fusion ? 2u : 0u) |
+                                  (args->flags & CLIFFT_GPU_SURVIVORS ? 4u : 0u) | (forced_meas ? 8u : 0u) |
+                                  (forced_faults ? 16u : 0u) | (args->flags & CLIFFT_GPU_TRACE ? 32u : 0u);
+        uint32_t group_req = args->group_threads;
+        std::vector<uint32_t> tune;
+        if (group_req == 0 && !(args->flags & CLIFFT_GPU_NO_AUTOTUNE)) {
+            std::lock_guard<std::mutex> lock(prog->tune_mu);
+            auto it = prog->tuned.find(tune_key);
+            if (it != prog->tuned.end())
+                group_req = it->second;
+            else if (shots >= kTuneMinShots)
+                tune = tune_candidates(*prog, args->precision);
+        }
+        LaunchPlan L = plan_launch(*prog, args->precision, group_req, shots, rec_words, det_words, obs_words,
+                                   allow_fusion);
         KParams K{};
         K.shots = shots;
         K.first_shot = args->first_shot;
@@ -578,21 +617,26 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         K.dust_eps = args->dust_eps > 0.0 ? args->dust_eps : (args->precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
         K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
                   (forced_meas ? KF_FORCED_MEAS : 0) | (forced_faults ? KF_FORCED_FAULTS : 0) |
-                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0) | (L.fuse ? KF_FUSE : 0);
-        K.fuse_bytes = L.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
-                                                                    : fuse_smem_bytes<double>())
-                               : 0;
+                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0);
         K.rec_words = rec_words;
         K.det_words = det_words;
         K.obs_words = obs_words;
         K.meas_out_words = (m.num_measurements + 63) / 64;
         K.det_out_words = (m.num_detectors + 63) / 64;
         K.obs_out_words = (m.num_observables + 63) / 64;
-        K.state_in_smem = L.state_in_smem ? 1 : 0;
-        K.state_stride = L.state_stride;
         const size_t amp = args->precision == CLIFFT_GPU_FP32 ? 8 : 16;
-        if (!L.state_in_smem)
-            K.state_global = buf.alloc(size_t(L.blocks) * L.regions * L.S * L.state_stride * amp);
+        // launch-shape dependent parameters (and the statevector slab)
+        auto apply_plan = [&](KParams& Kx, const LaunchPlan& Lx) {
+            Kx.flags = (K.flags & ~uint32_t(KF_FUSE)) | (Lx.fuse ? KF_FUSE : 0);
+            Kx.fuse_bytes = Lx.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
+                                                                          : fuse_smem_bytes<double>())
+                                     : 0;
+            Kx.state_in_smem = Lx.state_in_smem ? 1 : 0;
+            Kx.state_stride = Lx.state_stride;
+            Kx.state_global = Lx.state_in_smem
+                                  ? nullptr
+                                  : buf.alloc(size_t(Lx.blocks) * Lx.regions * Lx.S * Lx.state_stride * amp);
+        };
         const size_t n_counters = 5 + m.num_observables;
         const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;
         const size_t scratch_words = 2 + n_counters + (profile ? 8 : 0) + 8;
@@ -666,6 +710,49 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         cudaEvent_t e0, e1;
         CUDA_OK(cudaEventCreate(&e0));
         CUDA_OK(cudaEventCreate(&e1));
+        uint32_t launches = 0;
+        if (!tune.empty()) {
+            // Trial launches on the first shots of this call (their records are
+            // rewritten by the real launch below): up to two resident waves per
+            // candidate, fastest shots/s wins.
+            float best_rate = -1.f;
+            uint32_t best = 0;
+            for (uint32_t cand : tune) {
+                LaunchPlan Lc = plan_launch(*prog, args->precision, cand, shots, rec_words, det_words, obs_words,
+                                            allow_fusion);
+                const uint64_t wave = uint64_t(Lc.blocks) * Lc.regions * Lc.S;
+                const uint64_t trial = std::min<uint64_t>(shots, 2 * wave);
+                KParams Kc = K;
+                apply_plan(Kc, Lc);
+                Kc.shots = trial;
+                auto* sc = static_cast<unsigned long long*>(buf.alloc(scratch_words * 8 + 64));
+                CUDA_OK(cudaMemsetAsync(sc, 0, scratch_words * 8 + 64, st));
+                Kc.work_counter = sc;
+                Kc.error_word = reinterpret_cast<int*>(sc + 1);
+                Kc.counters = sc + 2;
+                Kc.phase_cycles = nullptr;
+                Kc.error_info = sc + scratch_words - 8;
+                CUDA_OK(cudaEventRecord(e0, st));
+                Lc.fn<<<Lc.blocks, Lc.threads, Lc.smem, st>>>(prog->dev, Kc);
+                CUDA_OK(cudaGetLastError());
+                CUDA_OK(cudaEventRecord(e1, st));
+                CUDA_OK(cudaEventSynchronize(e1));
+                ++launches;
+                float tms = 0.f;
+                CUDA_OK(cudaEventElapsedTime(&tms, e0, e1));
+                const float rate = float(trial) / std::max(tms, 1e-6f);
+                if (rate > best_rate) {
+                    best_rate = rate;
+                    best = cand;
+                }
+            }
+            {
+                std::lock_guard<std::mutex> lock(prog->tune_mu);
+                prog->tuned[tune_key] = best;
+            }
+            L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion);
+        }
+        apply_plan(K, L);
         CUDA_OK(cudaEventRecord(e0, st));
         L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
         CUDA_OK(cudaGetLastError());
@@ -716,7 +803,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->streamed_bytes = hs[6];
         if (out->observable_ones)
             for (uint32_t i = 0; i < m.num_observables; ++i) out->observable_ones[i] = hs[7 + i];
-        out->kernel_launches = 1;
+        out->kernel_launches = launches + 1;
         out->kernel_ms = ms;
         out->group_threads = L.G ? uint32_t(L.G) : uint32_t(L.threads);
         out->state_in_smem = L.state_in_smem ? 1u : 0u;

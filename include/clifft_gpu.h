@@ -63,6 +63,7 @@ extern "C" {
 #define CLIFFT_GPU_NO_FUSION 0x20u      /* plain executor: one statevector pass per opcode */
 #define CLIFFT_GPU_FORCE_FUSION 0x40u   /* reserved (fusion is on unless CLIFFT_GPU_NO_FUSION) */
 #define CLIFFT_GPU_PROFILE 0x80u        /* fill phase_cycles (adds timing atomics; not for benchmarks) */
+#define CLIFFT_GPU_NO_AUTOTUNE 0x100u   /* group_threads == 0: use the built-in heuristic, no trial launches */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
 
@@ -72,7 +73,8 @@ typedef struct clifft_gpu_sample_args {
     uint64_t first_shot;    /* global index of shot 0 (multi-GPU shards, resumption) */
     uint32_t precision;     /* CLIFFT_GPU_FP64 or CLIFFT_GPU_FP32 */
     uint32_t flags;
-    uint32_t group_threads; /* 0 = automatic; 1,2,4..32 = lanes per shot (32/G shots per warp); 64..1024 = one CTA per shot */
+    uint32_t group_threads; /* 0 = automatic (autotuned, see below); 1,2,4..32 = lanes per shot
+                               (32/G shots per warp); 64..1024 = one CTA of that size per shot */
     uint32_t reserved;
     double dust_eps;        /* relative dust threshold; 0 = 1e-18 (FP64) / 1e-9 (FP32) */
     /* CLIFFT_GPU_FORCED_MEAS: shots x total_meas_slots bytes (0/1) */
@@ -124,7 +126,15 @@ typedef struct clifft_gpu_outputs {
 int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out);
 /* Release a handle (waits for the device). */
 void clifft_gpu_free(clifft_gpu_program* prog);
-/* Sample. See the flags above for survivors / forced / trace behaviour. */
+/* Sample. See the flags above for survivors / forced / trace behaviour.
+ * Autotuning: with group_threads == 0 and no CLIFFT_GPU_NO_AUTOTUNE, the
+ * first call of a (precision, mode) pair on a program with at least 1024
+ * shots times a few candidate launch shapes (lanes per shot, or CTA size)
+ * on up to two resident waves of this call's own shots, keeps the fastest
+ * on the program handle, and uses it from then on. Results do not depend on
+ * the launch shape: every shot draws from its own Philox stream and every
+ * reduction has a fixed order. Trial launches are counted in
+ * kernel_launches but not in kernel_ms. */
 int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
                       clifft_gpu_outputs* out);
 /* "cuda:sm_100a" when a B200-class device is current; "unavailable:<why>" otherwise. */

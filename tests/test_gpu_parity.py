@@ -129,9 +129,11 @@ def test_launch_shape_independence(group):
                                amplitudes(ref["final_gamma"], ref["final_v"]), atol=1e-10)
 
 
+@pytest.mark.parametrize("group", [32, 512])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_large_k_global_state_forced_parity(precision):
-    # k = 17: 2^17 amplitudes per shot, state in a global slab (CTA per shot)
+def test_large_k_global_state_forced_parity(precision, group):
+    # k = 17: 2^17 amplitudes per shot in a global slab, one warp per shot
+    # (L2/HBM sweeps) or one CTA per shot (bulk-copy tile engine)
     prog = random_program(7, n=20, length=170, max_k=17, noise=False, classical=False,
                           expand_bias=0.5)
     assert prog.peak_rank >= 16
@@ -139,7 +141,8 @@ def test_large_k_global_state_forced_parity(precision):
     fm = np.zeros((4, prog.total_meas_slots), np.uint8)
     fm[:, :prog.num_measurements] = o["meas"]
     ref = O.run(prog, 4, forced_meas=fm, want_state=True)
-    g = forced_gpu(prog, fm, None, None, precision)
+    g = forced_gpu(prog, fm, None, None, precision, group)
+    assert g["group_threads"] == group and not g["state_in_smem"]
     assert np.array_equal(g["survived"].astype(bool), ref["reachable"].astype(bool))
     assert np.array_equal(g["final_k"], ref["final_k"])
     ptol = 1e-10 if precision == "fp64" else 1e-5
@@ -229,7 +232,7 @@ def test_fused_tile_sweeps_match_unfused(precision):
     faults, ros = unflatten(d)
     n = fm.shape[0]
     kw = dict(precision=precision, forced_meas=fm, faults=faults, readout_faults=ros, trace=True,
-              dump_shots=n)
+              dump_shots=n, group_threads=512)  # fusion is a feature of CTA groups (tile engine)
     a = cb.run(prog, n, 0, fusion=True, **kw)
     b = cb.run(prog, n, 0, fusion=False, **kw)
     assert a["fused"] and not b["fused"]
