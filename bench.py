@@ -1,26 +1,32 @@
 """Benchmark: shots/s of the Schrodinger-VM executor on the B200.
 
-Workload (one "step"): `sample_survivors` of the noisy 7x7 memory-grid
-program (n = 49, 10 rounds, DEPOLARIZE1/2 + X_ERROR at p = 1e-3, 12 magic
-gates, post-selection on all 240 detectors) for 10^6 shots per GPU, bytecode
-after the reference's own bytecode passes (tests/golden/programs/cfg1.npz,
-written by tests/golden/make_golden.py). Synthetic seeded data.
+Headline workload (one "step"): `sample` of the k = 24 program (random
+near-Clifford circuit, n = 64, 400 layers, 24 T gates, peak rank 24; bytecode
+after the reference's own bytecode passes, tests/golden/programs/cfg3.npz
+written by tests/golden/make_golden.py) for 296 shots per GPU, i.e. two
+resident waves of one CTA per SM with a 128 MiB complex-FP32 statevector each.
+Synthetic seeded data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl clifft_b200|reference]
 
-Reported `value` = survivor-sampled shots per second, whole job (sum over
-ranks, max-over-ranks device time), statevector in complex FP32 with FP64
-probability sums. `e2e` = the same metric through the public Python API
-(`clifft_b200.sample_survivors` on a freshly uploaded program, records read
-back to host numpy). `extras` carry the plain-FP64 executor on the same
-workload and the k = 10 / 16 / 24 programs side by side.
+`value` = shots per second of the batched FP32 executor (statevector in
+complex FP32, probability sums and renormalisation in FP64, fused tile sweeps,
+autotuned launch shape), whole job (sum over ranks, max-over-ranks device
+time). `e2e` = the same metric through the public Python API
+(`clifft_b200.sample` on a freshly uploaded program, records read back and
+unpacked on the host). `extras` put the plain FP64 executor (one pass per
+opcode, fixed launch heuristic) beside it on the same workload, the k = 10 and
+k = 16 programs, the noisy memory-grid survivor workload, and the largest
+FP32-vs-FP64 measurement-probability difference.
+
+`--impl reference` times the reference's own executor (oracle/_ref, built
+from the reference sources) on this host's cores on the same workload.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -31,8 +37,12 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PROGRAMS = os.path.join(ROOT, "tests", "golden", "programs")
-SHOTS_PER_GPU = 1_000_000
+HEADLINE = "cfg3"
+SHOTS_PER_GPU = 296  # two waves of 148 resident CTAs
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+METRIC = "shots/sec at k=10/16/24, FP32-batched vs FP64 GPU (1e-5 prob tol); HBM GB/s vs peak"
+WORKLOAD = ("cfg3: random near-Clifford n=64, 400 layers, 24 T, peak k=24 (2^24 amplitudes/shot); "
+            "clifft.sample, 296 shots per GPU per step")
 
 
 def measured_peaks():
@@ -56,7 +66,6 @@ class ClockSampler:
 
     def __init__(self, device_index: int):
         self.idx = device_index
-        self.proc = None
         self.lines = []
 
     def __enter__(self):
@@ -105,14 +114,20 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ GPU helpers
-def device_run(prog, dp, shots, seed, first_shot, precision, stream, bufs):
-    """One device-resident sampling step: program resident, outputs in HBM."""
+def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False):
+    """One device-resident sampling step: program resident, outputs in HBM.
+    plain = the plain executor: one pass per opcode, fixed heuristic launch
+    shape (no fusion, no autotuning)."""
     import ctypes
     from clifft_b200 import _native as N
+    flags = N.CLIFFT_GPU_DEVICE_PTRS
+    if survivors:
+        flags |= N.CLIFFT_GPU_SURVIVORS
+    if plain:
+        flags |= N.CLIFFT_GPU_NO_FUSION | N.CLIFFT_GPU_NO_AUTOTUNE
     a = N.SampleArgs(shots=shots, seed=seed, first_shot=first_shot,
                      precision=N.CLIFFT_GPU_FP32 if precision == "fp32" else N.CLIFFT_GPU_FP64,
-                     flags=N.CLIFFT_GPU_SURVIVORS | N.CLIFFT_GPU_DEVICE_PTRS,
-                     stream=stream.cuda_stream)
+                     flags=flags, stream=stream.cuda_stream)
     o = N.Outputs()
     for field, t in bufs.items():
         setattr(o, field, t.data_ptr() if t.numel() else None)
@@ -128,11 +143,12 @@ def output_buffers(torch, prog, shots, dev):
         "meas": torch.empty((shots, mw), dtype=torch.int64, device=dev),
         "det": torch.empty((shots, dw), dtype=torch.int64, device=dev),
         "obs": torch.empty((shots, ow), dtype=torch.int64, device=dev),
+        "exp_vals": torch.empty((shots, prog.num_exp_vals), dtype=torch.float64, device=dev),
         "survived": torch.empty(shots, dtype=torch.uint8, device=dev),
     }
 
 
-def time_device(torch, prog, shots, precision, steps, warmup, rank, flush):
+def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survivors=False, plain=False):
     import clifft_b200 as cb
     dev = torch.device("cuda", torch.cuda.current_device())
     dp = cb.load(prog)
@@ -140,14 +156,14 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush):
     bufs = output_buffers(torch, prog, shots, dev)
     first = rank * shots
     for w in range(warmup):
-        device_run(prog, dp, shots, 1000 + w, first, precision, stream, bufs)
+        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain)
     torch.cuda.synchronize()
-    times, kernel_ms, launches, passed, alg_bytes, groups = [], [], 0, 0, 0, set()
+    times, kernel_ms, launches, passed, alg_bytes, streamed, groups = [], [], 0, 0, 0, 0, set()
     for s in range(steps):
         flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        o = device_run(prog, dp, shots, 7 + s, first, precision, stream, bufs)
+        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain)
         ev1.record(stream)
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1))
@@ -155,23 +171,24 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush):
         launches += o.kernel_launches
         passed += o.passed_shots
         alg_bytes += o.algorithmic_bytes
+        streamed += o.streamed_bytes
         groups.add(o.group_threads)
     return {"ms": times, "kernel_ms": kernel_ms, "launches": launches, "passed": passed,
-            "alg_bytes": alg_bytes, "group_threads": sorted(groups)}
+            "alg_bytes": alg_bytes, "streamed_bytes": streamed, "group_threads": sorted(groups)}
 
 
-def time_e2e(prog_path, shots, steps, rank, torch):
+def time_e2e(name, shots, steps, torch):
     """Public-API path with host buffers: fresh upload of the program image
     (H2D), sampling, packed records read back (D2H) and unpacked to numpy."""
-    import numpy as np
     import clifft_b200 as cb
     from clifft_b200.program import Program
+    path = os.path.join(PROGRAMS, f"{name}.npz")
     times, h2d, d2h = [], 0, 0
     for s in range(steps + 1):
-        prog = Program.load(prog_path)  # host-side program, not yet on the device
+        prog = Program.load(path)  # host-side program, not yet on the device
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = cb.sample_survivors(prog, shots, seed=50 + s, keep_records=True, precision="fp32")
+        cb.sample(prog, shots, seed=50 + s, precision="fp32")
         dt = time.perf_counter() - t0
         if s == 0:
             continue  # first call pays one-time CUDA context / kernel attribute setup
@@ -179,57 +196,123 @@ def time_e2e(prog_path, shots, steps, rank, torch):
         h2d = cb.load(prog).device_bytes
         words = ((prog.num_measurements + 63) // 64 + (prog.num_detectors + 63) // 64 +
                  (prog.num_observables + 63) // 64)
-        d2h = shots * (words * 8 + 1) + 8 * (6 + prog.num_observables)
+        d2h = shots * (words * 8 + 1 + 8 * prog.num_exp_vals) + 8 * (6 + prog.num_observables)
         prog._device_program.free()
     return times, h2d, d2h
 
 
-def cpu_baseline(shots_hint=200_000, target_s=12.0):
-    """The reference executor (oracle/_ref) on this host's cores, shot-parallel,
-    on a bounded sample of the workload; falls back to the C oracle port."""
+def prob_error(name, shots=8):
+    """Largest |p_FP32 - p_FP64| over every measurement of `shots` forced
+    trajectories (outcomes from an FP64 run of the same program)."""
+    import numpy as np
+    import clifft_b200 as cb
+    prog = load_program(name)
+    f = cb.run(prog, shots, 5, precision="fp64", trace=True)
+    words = f["meas_words"]
+    bits = np.unpackbits(words.view(np.uint8), axis=1, bitorder="little")[:, :prog.num_measurements]
+    fm = np.zeros((shots, prog.total_meas_slots), np.uint8)
+    fm[:, :prog.num_measurements] = bits
+    a = cb.run(prog, shots, 0, precision="fp64", forced_meas=fm, trace=True)
+    b = cb.run(prog, shots, 0, precision="fp32", forced_meas=fm, trace=True)
+    pa, pb = np.nan_to_num(a["meas_prob"]), np.nan_to_num(b["meas_prob"])
+    return float(np.max(np.abs(pa - pb))) if pa.size else 0.0
+
+
+# ------------------------------------------------------------ CPU reference
+def ref_modes(prog, cores, budget_s):
+    """The reference executor on this host: shot-parallel (one std::thread per
+    core, OpenMP team of 1) and intra-shot (one thread, OpenMP team of all
+    cores, the executor's own large-k parallelism). Returns [(mode, shots/s,
+    shots, seconds)] with each sample sized to about budget_s seconds."""
     from oracle import pyoracle as O
-    prog = load_program("cfg1")
+    out = []
+    surv = bool(prog.has_postselection)
+    for mode, thr, omp in (("shot-parallel", cores, 1), ("intra-shot OpenMP", 1, cores)):
+        n = max(thr, 2)
+        t = O.ref_time_sample(prog, n, 3, thr, surv, omp)
+        n = int(max(n, min(50_000_000, n * budget_s / max(t, 1e-3))))
+        n = max(thr, (n // thr) * thr)
+        t = O.ref_time_sample(prog, n, 4, thr, surv, omp)
+        out.append((mode, n / t, n, t))
+    return out
+
+
+def cpu_baseline(name):
+    from oracle import pyoracle as O
+    prog = load_program(name)
     cores = len(os.sched_getaffinity(0))
     if O.ref_available():
-        probe = 20_000
-        t = O.ref_time_sample(prog, probe, 3, cores, True)
-        n = int(min(5_000_000, max(probe, probe * target_s / max(t, 1e-3))))
-        t = O.ref_time_sample(prog, n, 4, cores, True)
-        return {"value": n / t, "unit": "shots/s", "cores": cores, "kind": "reference",
-                "sample": f"{n} shots of the cfg1 program, {cores} threads x clifft::sample_survivors "
-                          f"(oracle/_ref, dispatch {O.ref_backend()})"}
-    n = 20_000
+        modes = ref_modes(prog, cores, 6.0)
+        best = max(modes, key=lambda m: m[1])
+        t1 = O.ref_time_sample(prog, 2, 5, 1, bool(prog.has_postselection), 1)
+        desc = "; ".join(f"{m}: {n} shots in {t:.1f} s = {v:.3g}/s" for m, v, n, t in modes)
+        return {"value": best[1], "unit": "shots/s", "cores": cores, "kind": "reference",
+                "sample": f"{name} program, reference clifft::sample built from its sources (oracle/_ref, "
+                          f"dispatch {O.ref_backend()}); best of [{desc}]; 1 core: {2 / t1:.3g}/s"}
+    n = 2
     t0 = time.perf_counter()
     O.run(prog, n, seed=3, rng=O.RNG_XOSHIRO)
     t = time.perf_counter() - t0
     return {"value": n / t, "unit": "shots/s", "cores": 1, "kind": "port",
-            "sample": f"{n} shots of the cfg1 program through the C oracle, 1 thread"}
+            "sample": f"{n} shots of the {name} program through the C oracle, 1 thread"}
 
 
-def k_sweep(torch, flush):
-    """FP32 vs FP64 shots/s on the k = 10 / 16 / 24 programs (configs 2 and 3)."""
-    import numpy as np
+def reference_arm(args, config):
+    from oracle import pyoracle as O
+    prog = load_program(HEADLINE)
+    cores = len(os.sched_getaffinity(0))
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference executor (oracle/_ref) not built on this machine"}))
+        return
+    # the faster of the reference's two parallel modes on a short probe
+    modes = ref_modes(prog, cores, 2.0)
+    mode = max(modes, key=lambda m: m[1])[0]
+    thr, omp = (cores, 1) if mode == "shot-parallel" else (1, cores)
+    per_step = 4 * cores
+    for w in range(args.warmup):
+        O.ref_time_sample(prog, thr, 900 + w, thr, False, omp)
+    ts = [O.ref_time_sample(prog, per_step, 10 + s, thr, False, omp) for s in range(args.steps)]
+    ms = 1e3 * sum(ts) / len(ts)
+    val = per_step / (ms / 1e3)
+    line = {"metric": METRIC, "value": val, "unit": "shots/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128 state / f64", "data": "synthetic", "config": config,
+            "impl": "reference",
+            "cpu_baseline": {"value": val, "unit": "shots/s", "cores": cores, "kind": "reference",
+                             "sample": f"{per_step} shots per step of the {HEADLINE} program, {mode} "
+                                       f"({thr} threads x OpenMP team {omp}), reference clifft::sample "
+                                       f"(oracle/_ref)"},
+            "e2e": {"value": val, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def k_sweep(torch, flush, head_fp32, head_fp64):
+    """Batched FP32 vs plain FP64 shots/s on the k = 10 / 16 programs of the
+    multi-program set (seeds 100..163) plus the k = 24 headline numbers."""
     from clifft_b200.program import Program
-    out = {}
     peaks = {}
     for name in sorted(os.listdir(PROGRAMS)):
         if name.startswith("cfg2_"):
             p = Program.load(os.path.join(PROGRAMS, name))
             peaks.setdefault(p.peak_rank, name[:-4])
-    picks = [(10, peaks.get(10), 10_000), (16, peaks.get(16), 10_000), (24, "cfg3", 256)]
-    for k, name, shots in picks:
+    out = {}
+    for k, name, shots in ((10, peaks.get(10), 10_000), (16, peaks.get(16), 10_000)):
         if name is None:
             continue
         prog = load_program(name)
         row = {"program": name, "shots": shots}
-        for prec in ("fp32", "fp64"):
-            r = time_device(torch, prog, shots, prec, steps=2, warmup=1, rank=0, flush=flush)
-            ms = min(r["ms"])
+        for prec, plain in (("fp32", False), ("fp64", True)):
+            r = time_device(torch, prog, shots, prec, steps=2, warmup=2, rank=0, flush=flush, plain=plain)
             kms = min(r["kernel_ms"])
-            row[f"{prec}_shots_per_s"] = shots / (ms / 1e3)
-            row[f"{prec}_kernel_GBps"] = (r["alg_bytes"] / len(r["ms"])) / (kms / 1e3) / 1e9
-        row["fp32_over_fp64"] = row["fp32_shots_per_s"] / row["fp64_shots_per_s"]
+            key = "fp32_batched" if prec == "fp32" else "fp64_plain"
+            row[f"{key}_shots_per_s"] = shots / (min(r["ms"]) / 1e3)
+            row[f"{key}_alg_GBps"] = (r["alg_bytes"] / len(r["ms"])) / (kms / 1e3) / 1e9
+            row[f"{key}_group_threads"] = r["group_threads"]
+        row["fp32_over_fp64"] = row["fp32_batched_shots_per_s"] / row["fp64_plain_shots_per_s"]
         out[f"k{k}"] = row
+    out["k24"] = {"program": HEADLINE, "shots": SHOTS_PER_GPU, "fp32_batched_shots_per_s": head_fp32,
+                  "fp64_plain_shots_per_s": head_fp64, "fp32_over_fp64": head_fp32 / head_fp64}
     return out
 
 
@@ -246,54 +329,32 @@ def main():
                          "(for ncu captures); prints one summary line")
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--plain", action="store_true", help="with --profile: the plain executor")
     args = ap.parse_args()
     if args.profile:
         import torch
         torch.cuda.set_device(0)
         prog = load_program(args.profile)
         flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-        r = time_device(torch, prog, args.shots, args.precision, args.steps, args.warmup, 0, flush)
+        r = time_device(torch, prog, args.shots, args.precision, args.steps, args.warmup, 0, flush,
+                        survivors=bool(prog.has_postselection), plain=args.plain)
         print(json.dumps({"program": args.profile, "shots": args.shots, "precision": args.precision,
-                          "ms": r["ms"], "kernel_ms": r["kernel_ms"], "alg_bytes": r["alg_bytes"],
+                          "plain": args.plain, "ms": r["ms"], "kernel_ms": r["kernel_ms"],
+                          "alg_bytes": r["alg_bytes"], "streamed_bytes": r["streamed_bytes"],
                           "launches": r["launches"], "group_threads": r["group_threads"]}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    config = {"workload": "cfg1: 7x7 noisy memory grid, n=49, 10 rounds, p=1e-3, 12 magic, "
-                          "post-select all 240 detectors; sample_survivors",
-              "shots_per_gpu_per_step": SHOTS_PER_GPU, "global_batch_shots": SHOTS_PER_GPU * world,
-              "peak_k": None, "parallelism": f"shot-sharded x{world}",
-              "l2": "256 MiB buffer zeroed between timed steps (inputs are on-chip sized)"}
+    config = {"workload": WORKLOAD, "shots_per_gpu_per_step": SHOTS_PER_GPU,
+              "global_batch_shots": SHOTS_PER_GPU * world, "peak_k": 24,
+              "parallelism": f"shot-sharded x{world}",
+              "l2": "statevectors (128 MiB each, 148 resident) far exceed L2; a 256 MiB buffer is also "
+                    "zeroed between timed steps"}
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        from oracle import pyoracle as O
-        prog = load_program("cfg1")
-        config["peak_k"] = prog.peak_rank
-        cores = len(os.sched_getaffinity(0))
-        if not O.ref_available():
-            print(json.dumps({"impl": "reference", "unavailable":
-                              "reference harness oracle/_ref not built on this machine"}))
-            return
-        per_step = 200_000
-        for w in range(args.warmup):
-            O.ref_time_sample(prog, 20_000, 900 + w, cores, True)
-        ts = [O.ref_time_sample(prog, per_step, 10 + s, cores, True) for s in range(args.steps)]
-        ms = 1e3 * sum(ts) / len(ts)
-        val = per_step / (ms / 1e3)
-        line = {"metric": "survivor-sampled shots/s (cfg1 memory grid, FP64 reference executor)",
-                "value": val, "unit": "shots/s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config, "impl": "reference",
-                "cpu_baseline": {"value": val, "unit": "shots/s", "cores": cores, "kind": "reference",
-                                 "sample": f"{per_step} shots per step, {cores} threads x "
-                                           f"clifft::sample_survivors (oracle/_ref)"},
-                "e2e": {"value": val, "unit": "shots/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        if rank == 0:
+            reference_arm(args, config)
         return
 
     import torch
@@ -307,7 +368,7 @@ def main():
     import clifft_b200 as cb
     if not cb.backend_name().startswith("cuda:sm_100a"):
         raise SystemExit(f"no sm_100 device: {cb.backend_name()}")
-    prog = load_program("cfg1")
+    prog = load_program(HEADLINE)
     config["peak_k"] = prog.peak_rank
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
@@ -322,30 +383,30 @@ def main():
         barrier()
         r = time_device(torch, prog, SHOTS_PER_GPU, "fp32", args.steps, args.warmup, rank, flush)
         barrier()
-    total_ms = sum(r["ms"])
-    step_ms = total_ms / args.steps
-    passed = r["passed"]
+    step_ms = sum(r["ms"]) / args.steps
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([step_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         step_ms = float(t.item())
-        pt = torch.tensor([passed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(pt, op=dist.ReduceOp.SUM)
-        passed = int(pt.item())
     value = SHOTS_PER_GPU * world / (step_ms / 1e3)
 
-    # roofline of the sampling kernel (device time from events inside the call)
+    # roofline of the sampling kernel: algorithmic statevector bytes of one
+    # launch / its device time (CUDA events on the launching stream, recorded
+    # inside the library)
     peak, peak_kind = measured_peaks()
     kms = sum(r["kernel_ms"]) / len(r["kernel_ms"])
     bytes_per_launch = r["alg_bytes"] / args.steps
     achieved = bytes_per_launch / (kms / 1e3) / 1e9
+    streamed_gbps = (r["streamed_bytes"] / args.steps) / (kms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get("cfg1_fp32_dram_bytes_per_launch")
+                per_shot = json.load(f).get("cfg3_fp32_dram_bytes_per_shot")
+            if per_shot:
+                traffic = per_shot * SHOTS_PER_GPU
         except Exception:
             traffic = None
 
@@ -353,35 +414,43 @@ def main():
     e2e = None
     cpu = None
     if rank == 0:
-        e_times, h2d, d2h = time_e2e(os.path.join(PROGRAMS, "cfg1.npz"), SHOTS_PER_GPU,
-                                     max(2, min(args.steps, 3)), rank, torch)
+        e_times, h2d, d2h = time_e2e(HEADLINE, SHOTS_PER_GPU, max(2, min(args.steps, 3)), torch)
         e2e = {"value": SHOTS_PER_GPU / (sum(e_times) / len(e_times)), "unit": "shots/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": 1e3 * sum(e_times) / len(e_times)}
         if not args.no_extras:
-            r64 = time_device(torch, prog, SHOTS_PER_GPU, "fp64", 2, 1, 0, flush)
-            extras["fp64_plain_executor_shots_per_s"] = SHOTS_PER_GPU / (min(r64["ms"]) / 1e3)
-            extras["fp32_over_fp64"] = value / world / extras["fp64_plain_executor_shots_per_s"]
-            extras["k_sweep"] = k_sweep(torch, flush)
-        world_cpu = world == 1
-        if world_cpu:
-            cpu = cpu_baseline()
+            r64 = time_device(torch, prog, SHOTS_PER_GPU, "fp64", 2, 1, 0, flush, plain=True)
+            fp64 = SHOTS_PER_GPU / (min(r64["ms"]) / 1e3)
+            extras["fp64_plain_executor_shots_per_s"] = fp64
+            extras["fp64_plain_alg_GBps"] = (r64["alg_bytes"] / 2) / (min(r64["kernel_ms"]) / 1e3) / 1e9
+            extras["fp32_over_fp64"] = (value / world) / fp64
+            extras["fp32_streamed_GBps"] = streamed_gbps
+            extras["k_sweep"] = k_sweep(torch, flush, value / world, fp64)
+            c1 = load_program("cfg1")
+            r1 = time_device(torch, c1, 1_000_000, "fp32", 2, 2, 0, flush, survivors=True)
+            r1p = time_device(torch, c1, 1_000_000, "fp64", 2, 1, 0, flush, survivors=True, plain=True)
+            extras["memory_grid_survivors"] = {
+                "program": "cfg1 (7x7 noisy memory grid, post-selected on all detectors)",
+                "shots": 1_000_000, "fp32_batched_shots_per_s": 1e9 / min(r1["ms"]),
+                "fp64_plain_shots_per_s": 1e9 / min(r1p["ms"]), "survivors_per_step": r1["passed"] / 2}
+            extras["max_abs_prob_diff_fp32_vs_fp64"] = {
+                "k24": prob_error(HEADLINE, 8), "k16": prob_error(extras["k_sweep"]["k16"]["program"], 64)}
+        if world == 1:
+            cpu = cpu_baseline(HEADLINE)
     line = {
-        "metric": "survivor-sampled shots/s (cfg1 memory grid, batched FP32 statevector, FP64 sums)",
+        "metric": METRIC,
         "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 state / f64 reductions",
         "data": "synthetic (seeded generator, reference bytecode passes)",
         "config": config,
-        "survivors_per_step": passed / args.steps,
         "gpu_launches": r["launches"],
         "group_threads": r["group_threads"],
         "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "note": f"algorithmic statevector bytes / kernel time; peak {peak_kind}; "
-                             "statevectors are shared-memory resident at this k, so frac > 1 "
-                             "means on-chip, not HBM"},
+                     "note": f"algorithmic statevector bytes per launch / kernel time (peak {peak_kind}); "
+                             f"bytes actually streamed after fusion: {streamed_gbps:.0f} GB/s"},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "extras": extras,

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <tuple>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -248,10 +249,52 @@ struct clifft_gpu_program {
     size_t blob_bytes = 0;
     std::vector<uint8_t> expected_host;
     int device = 0;
-    // launch shapes picked by the autotuner, per (precision, mode) key
-    std::mutex tune_mu;
-    std::map<uint32_t, uint32_t> tuned;
+    uint64_t content_hash = 0;  // FNV-1a of the device image and the launch-relevant counts
+    // Statevector slab kept between calls (mapping tens of GB afresh on every
+    // call costs more than a large-k launch's own setup). One call at a time
+    // holds it; a concurrent call on the same handle allocates its own.
+    std::mutex slab_mu;
+    void* slab = nullptr;
+    size_t slab_bytes = 0;
+    bool slab_busy = false;
 };
+
+namespace {
+
+// A call's use of the program's statevector slab: the first request takes the
+// cached slab (growing it if needed); later requests of the same call reuse
+// it, since the call's launches run one after another on one stream.
+struct SlabLease {
+    clifft_gpu_program& prog;
+    StreamBuffers& fallback;
+    cudaStream_t stream;
+    bool held = false;
+    explicit SlabLease(clifft_gpu_program& p, StreamBuffers& b, cudaStream_t s) : prog(p), fallback(b), stream(s) {}
+    void* get(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        if (held && prog.slab_bytes >= bytes) return prog.slab;
+        std::lock_guard<std::mutex> lock(prog.slab_mu);
+        if (!held && prog.slab_busy) return fallback.alloc(bytes);  // another call holds it
+        prog.slab_busy = held = true;
+        if (prog.slab_bytes < bytes) {
+            CUDA_OK(cudaStreamSynchronize(stream));  // earlier launches of this call may use the old slab
+            if (prog.slab) cudaFree(prog.slab);
+            prog.slab = nullptr;
+            prog.slab_bytes = 0;
+            CUDA_OK(cudaMalloc(&prog.slab, bytes));
+            prog.slab_bytes = bytes;
+        }
+        return prog.slab;
+    }
+    ~SlabLease() {
+        if (!held) return;
+        cudaStreamSynchronize(stream);  // no launch of this call may still use it
+        std::lock_guard<std::mutex> lock(prog.slab_mu);
+        prog.slab_busy = false;
+    }
+};
+
+}  // namespace
 
 namespace {
 
@@ -283,8 +326,9 @@ struct LaunchPlan {
     bool state_in_smem;
     uint64_t state_stride;
     uint32_t nw_words;
-    bool tiles;  // statevector passes stream through the bulk-copy tile engine
-    bool fuse;   // ... and consecutive opcodes fuse into one pass
+    bool tiles;       // statevector passes stream through the bulk-copy tile engine
+    bool fuse;        // ... and consecutive opcodes fuse into one pass
+    uint32_t stages;  // tile buffers per CTA (3 lets two 256-thread CTAs share an SM)
 };
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
@@ -333,7 +377,7 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     auto region_bytes = [&](bool in_smem) {
         size_t fuse = 0;  // tile-engine scratch: every CTA group with a global-memory statevector
         if (G == 0 && !in_smem)
-            fuse = precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>() : fuse_smem_bytes<double>();
+            fuse = precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(L.stages) : fuse_smem_bytes<double>(L.stages);
         return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
                ~size_t(15);
     };
@@ -348,9 +392,11 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
             L.threads = L.regions * 32;
         }
     } else {
-        int t = group_req > 32 ? int(group_req) : (state_bytes <= (size_t(32) << 10) ? 256 : 512);
+        // default: 256 threads, so two CTAs (three tile buffers each) share an SM
+        int t = group_req > 32 ? int(group_req) : 256;
         L.threads = std::min(t, max_threads);
         L.regions = 1;
+        L.stages = L.threads <= 256 ? 3 : 4;
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
     L.tiles = G == 0 && !L.state_in_smem;
@@ -381,8 +427,9 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
 
 // Launch shapes the autotuner tries (group_threads encoding): sub-warp groups
 // around the heuristic width for shared-memory statevectors, warp or CTA
-// groups for L2/HBM-resident ones up to 4 MiB. Larger statevectors have one
-// sensible shape (a CTA streaming tiles) and are not tuned.
+// groups for L2/HBM-resident ones up to 4 MiB, and for larger statevectors a
+// 512-thread CTA with four tile buffers against two 256-thread CTAs per SM
+// with three each.
 std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t precision) {
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const size_t state_bytes = (size_t(1) << p.meta.peak_rank) * amp;
@@ -393,11 +440,23 @@ std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t prec
             if (x >= 1 && x <= 32) c.push_back(uint32_t(x));
     } else if (state_bytes <= (size_t(4) << 20)) {
         c = {32, 16, 256, 512};
+    } else {
+        c = {256, 512};
     }
     return c;
 }
 
 constexpr uint64_t kTuneMinShots = 1024;
+
+// Launch shapes picked by the autotuner, shared by every handle of the same
+// program content in this process: (content hash, device, precision/mode).
+std::mutex g_tune_mu;
+std::map<std::tuple<uint64_t, int, uint32_t>, uint32_t> g_tuned;
+
+uint64_t fnv1a(const uint8_t* p, size_t n, uint64_t h = 1469598103934665603ull) {
+    for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return h;
+}
 
 }  // namespace
 
@@ -483,6 +542,12 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
         size_t o_exo = b.put(p->expected_host.data(), p->expected_host.size());
         b.bytes.resize(b.bytes.size() + 256);
         CUDA_OK(cudaGetDevice(&p->device));
+        {
+            const uint32_t counts[] = {im.peak_rank, im.num_measurements, im.total_meas_slots, im.num_detectors,
+                                       im.num_observables, im.num_exp_vals, im.num_words, im.num_instructions};
+            p->content_hash = fnv1a(reinterpret_cast<const uint8_t*>(counts), sizeof(counts),
+                                    fnv1a(b.bytes.data(), b.bytes.size()));
+        }
         CUDA_OK(cudaMalloc(&p->blob, b.bytes.size()));
         p->blob_bytes = b.bytes.size();
         CUDA_OK(cudaMemcpy(p->blob, b.bytes.data(), b.bytes.size(), cudaMemcpyHostToDevice));
@@ -536,9 +601,10 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
 
 void clifft_gpu_free(clifft_gpu_program* prog) {
     if (!prog) return;
-    if (prog->blob) {
+    if (prog->blob || prog->slab) {
         cudaDeviceSynchronize();
-        cudaFree(prog->blob);
+        if (prog->blob) cudaFree(prog->blob);
+        if (prog->slab) cudaFree(prog->slab);
     }
     delete prog;
 }
@@ -574,6 +640,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         CUDA_OK(cudaSetDevice(prog->device));
         cudaStream_t st = static_cast<cudaStream_t>(args->stream);
         StreamBuffers buf(st);
+        SlabLease slab(*prog, buf, st);
 
         // host-side validation of forced-fault inputs (bounds only)
         std::vector<uint32_t> h_foff, h_roff;
@@ -600,10 +667,11 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
                                   (forced_faults ? 16u : 0u) | (args->flags & CLIFFT_GPU_TRACE ? 32u : 0u);
         uint32_t group_req = args->group_threads;
         std::vector<uint32_t> tune;
+        const auto tune_id = std::make_tuple(prog->content_hash, prog->device, tune_key);
         if (group_req == 0 && !(args->flags & CLIFFT_GPU_NO_AUTOTUNE)) {
-            std::lock_guard<std::mutex> lock(prog->tune_mu);
-            auto it = prog->tuned.find(tune_key);
-            if (it != prog->tuned.end())
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            auto it = g_tuned.find(tune_id);
+            if (it != g_tuned.end())
                 group_req = it->second;
             else if (shots >= kTuneMinShots)
                 tune = tune_candidates(*prog, args->precision);
@@ -628,14 +696,15 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         // launch-shape dependent parameters (and the statevector slab)
         auto apply_plan = [&](KParams& Kx, const LaunchPlan& Lx) {
             Kx.flags = (K.flags & ~uint32_t(KF_FUSE)) | (Lx.fuse ? KF_FUSE : 0);
-            Kx.fuse_bytes = Lx.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>()
-                                                                          : fuse_smem_bytes<double>())
+            Kx.fuse_bytes = Lx.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(Lx.stages)
+                                                                          : fuse_smem_bytes<double>(Lx.stages))
                                      : 0;
+            Kx.stages = Lx.stages;
             Kx.state_in_smem = Lx.state_in_smem ? 1 : 0;
             Kx.state_stride = Lx.state_stride;
             Kx.state_global = Lx.state_in_smem
                                   ? nullptr
-                                  : buf.alloc(size_t(Lx.blocks) * Lx.regions * Lx.S * Lx.state_stride * amp);
+                                  : slab.get(size_t(Lx.blocks) * Lx.regions * Lx.S * Lx.state_stride * amp);
         };
         const size_t n_counters = 5 + m.num_observables;
         const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;
@@ -747,8 +816,8 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
                 }
             }
             {
-                std::lock_guard<std::mutex> lock(prog->tune_mu);
-                prog->tuned[tune_key] = best;
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                g_tuned[tune_id] = best;
             }
             L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion);
         }

@@ -122,6 +122,7 @@ struct KParams {
     double* out_final_v;
     uint64_t dump_shots;
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
+    uint32_t stages;      // tile buffers per CTA (2..kMaxStages) when fuse_bytes != 0
     unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
 };
 
@@ -382,16 +383,22 @@ struct MicroOp {
     double c[32];   // up to 16 complex coefficients
 };
 constexpr int kMaxMicroOps = 24;
-constexpr int kStages = 4;         // tiles in flight per CTA
+constexpr int kMaxStages = 4;      // tile buffers (tiles in flight) per CTA: 2..4, chosen per launch
 constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 template <typename R>
 struct TileCfg {
     static constexpr int kBits = sizeof(R) == 4 ? 12 : 11;  // 32 KiB per tile buffer
 };
+// Tile-engine scratch of one CTA: [kMaxStages mbarriers][micro-ops][64 run
+// offsets][64-byte axis -> local bit table][stages tile buffers, 128-B aligned]
+constexpr uint32_t kFuseBarOffset = 0;
+constexpr uint32_t kFuseMopsOffset = kMaxStages * 8u;
+constexpr uint32_t kFuseTablesOffset = kFuseMopsOffset + kMaxMicroOps * (uint32_t)sizeof(MicroOp);
+constexpr uint32_t kFuseLbitOffset = kFuseTablesOffset + 64u * 8u;
+constexpr uint32_t kFuseBufOffset = (kFuseLbitOffset + 64u + 127u) & ~127u;
 template <typename R>
-__host__ __device__ constexpr uint32_t fuse_smem_bytes() {
-    return (uint32_t)(kStages * (1u << TileCfg<R>::kBits) * 2u * sizeof(R) + kStages * 8u +
-                      kMaxMicroOps * sizeof(MicroOp) + 64u * 8u + 64u + 64u);
+__host__ __device__ constexpr uint32_t fuse_smem_bytes(uint32_t stages) {
+    return kFuseBufOffset + stages * (1u << TileCfg<R>::kBits) * 2u * (uint32_t)sizeof(R);
 }
 
 // ---- bulk-copy (TMA, untiled) and mbarrier primitives. Every copy here reads
@@ -673,16 +680,10 @@ struct Shot {
     __device__ __forceinline__ uint8_t local_bit(uint32_t axis) const {
         return reinterpret_cast<const uint8_t*>(fuse + fuse_lbit_offset())[axis];
     }
-    // fused-sweep scratch: [kStages tile buffers][kStages mbarriers][micro-ops]
-    // [64 run offsets][64-byte axis -> local bit table]
-    static __host__ __device__ constexpr uint32_t fuse_bar_offset() {
-        return kStages * (1u << TileCfg<R>::kBits) * (uint32_t)sizeof(T);
-    }
-    static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return fuse_bar_offset() + kStages * 8u; }
-    static __host__ __device__ constexpr uint32_t fuse_tables_offset() {
-        return fuse_mops_offset() + kMaxMicroOps * (uint32_t)sizeof(MicroOp);
-    }
-    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return fuse_tables_offset() + 64u * 8u; }
+    static __host__ __device__ constexpr uint32_t fuse_bar_offset() { return kFuseBarOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return kFuseMopsOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_tables_offset() { return kFuseTablesOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return kFuseLbitOffset; }
     __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
                                          int nc) {
         if (Grp::rank() == 0) {
@@ -1526,7 +1527,7 @@ struct Shot {
     // tile t covers the run offsets `runoff` (shared table, 2^(TILE_BITS - r)
     // runs of 2^r amplitudes) shifted by pdep(t, C). Loads come from
     // v[load_add + ...], optional stores (the first `store_runs` runs of each
-    // tile) go to v[store_add + ...]. Bulk copies (TMA) run kStages tiles
+    // tile) go to v[store_add + ...]. Bulk copies (TMA) run K.stages tiles
     // ahead; `compute(buf, t)` is called by every thread and must synchronise
     // the CTA before it returns. Returns false after a barrier timeout.
     uint32_t cur_pc = 0;   // instruction being executed (diagnostics)
@@ -1536,8 +1537,9 @@ struct Shot {
                                  uint32_t store_runs, Compute compute) {
         constexpr uint32_t MB = TileCfg<R>::kBits;
         constexpr uint32_t TN = 1u << MB;
-        T* bufs = reinterpret_cast<T*>(fuse);
+        T* bufs = reinterpret_cast<T*>(fuse + kFuseBufOffset);
         uint64_t* bars = reinterpret_cast<uint64_t*>(fuse + fuse_bar_offset());
+        const uint32_t nst = K.stages;
         const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
         const uint32_t nruns = 1u << (MB - r);
         const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
@@ -1554,7 +1556,7 @@ struct Shot {
         fence_async_global();
         __syncthreads();
         auto issue_load = [&](uint64_t t) {
-            const uint32_t st = (uint32_t)(t % kStages);
+            const uint32_t st = (uint32_t)(t % nst);
             const uint64_t base = load_add + pdep(t, C);
             if (lane == 0) mbar_expect_tx(&bars[st], TN * (uint32_t)sizeof(T));
             __syncwarp();
@@ -1562,12 +1564,12 @@ struct Shot {
                 bulk_load(bufs + st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[st]);
         };
         if (warp == 0)
-            for (uint64_t t = 0; t < ntiles && t < (uint64_t)(kStages - 1); ++t) issue_load(t);
+            for (uint64_t t = 0; t < ntiles && t < (uint64_t)(nst - 1); ++t) issue_load(t);
         bool ok_all = true;
         long long waited = 0;
         uint64_t t = 0;
         for (; t < ntiles; ++t) {
-            const uint32_t st = (uint32_t)(t % kStages);
+            const uint32_t st = (uint32_t)(t % nst);
             const uint32_t parity = (phase >> st) & 1u;
             uint32_t ok = 0;
             const long long w0 = clock64();
@@ -1590,10 +1592,10 @@ struct Shot {
                     bulk_commit();
                 }
             }
-            if (warp == 0 && t + kStages - 1 < ntiles) {
+            if (warp == 0 && t + nst - 1 < ntiles) {
                 if (store_runs) bulk_wait_read1();  // the stage being refilled held tile t-1
                 __syncwarp();
-                issue_load(t + kStages - 1);
+                issue_load(t + nst - 1);
             }
         }
         if (!ok_all) {
@@ -1605,11 +1607,11 @@ struct Shot {
                 K.error_info[3] = ntiles;
                 K.error_info[4] = r;
                 K.error_info[5] = k;
-                K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[t % kStages]);
+                K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[t % nst]);
                 K.error_info[7] = (unsigned long long)waited;
             }
-            for (uint64_t q = t; q < ntiles && q < t + kStages - 1; ++q) {
-                const uint32_t st = (uint32_t)(q % kStages);
+            for (uint64_t q = t; q < ntiles && q < t + nst - 1; ++q) {
+                const uint32_t st = (uint32_t)(q % nst);
                 for (uint32_t it = 0; it < (1u << 20); ++it)
                     if (mbar_try_wait(&bars[st], (phase >> st) & 1u)) break;
                 phase ^= 1u << st;
@@ -2121,7 +2123,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
         // of every shot this CTA runs
         if (threadIdx.x == 0) {
             uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW>::fuse_bar_offset());
-            for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
+            for (int st = 0; st < kMaxStages; ++st) mbar_init(&bars[st], 1);
             mbar_fence_init();
         }
         __syncthreads();

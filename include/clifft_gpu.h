@@ -28,7 +28,11 @@
  *
  * Every entry point returns 0 on success or a negative status and never throws
  * across the ABI. Calls are re-entrant: each call uses its own stream-ordered
- * scratch, so concurrent host threads may sample the same program.
+ * scratch, so concurrent host threads may sample the same program. A sampling
+ * call returns after its stream has finished the call's work. Statevectors
+ * that do not fit in shared memory live in a device slab kept on the program
+ * handle between calls (one call at a time uses it; a concurrent call
+ * allocates its own for the call's duration).
  */
 #ifndef CLIFFT_GPU_H
 #define CLIFFT_GPU_H
@@ -124,14 +128,16 @@ typedef struct clifft_gpu_outputs {
 
 /* Upload + validate a program. *out receives an opaque handle. */
 int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out);
-/* Release a handle (waits for the device). */
+/* Release a handle (waits for the device) and the statevector slab that
+ * sampling calls keep on it between calls. */
 void clifft_gpu_free(clifft_gpu_program* prog);
 /* Sample. See the flags above for survivors / forced / trace behaviour.
  * Autotuning: with group_threads == 0 and no CLIFFT_GPU_NO_AUTOTUNE, the
  * first call of a (precision, mode) pair on a program with at least 1024
  * shots times a few candidate launch shapes (lanes per shot, or CTA size)
  * on up to two resident waves of this call's own shots, keeps the fastest
- * on the program handle, and uses it from then on. Results do not depend on
+ * for every handle of the same program content on this device (for the rest
+ * of the process), and uses it from then on. Results do not depend on
  * the launch shape: every shot draws from its own Philox stream and every
  * reduction has a fixed order. Trial launches are counted in
  * kernel_launches but not in kernel_ms. */

@@ -93,6 +93,9 @@ def ref_lib():
         lib.ref_time_sample.restype = ctypes.c_double
         lib.ref_time_sample.argtypes = [P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                         ctypes.c_int]
+        lib.ref_time_sample_omp.restype = ctypes.c_double
+        lib.ref_time_sample_omp.argtypes = [P, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int]
         lib.ref_forced_run.restype = ctypes.c_int
         lib.ref_forced_run.argtypes = [P, ctypes.c_uint32] + [P] * 19
         lib.ref_run_passes.restype = P
@@ -220,9 +223,15 @@ def ref_sample_survivors(prog, shots: int, seed: int, keep_records: bool = False
     return res
 
 
-def ref_time_sample(prog, shots: int, seed: int, threads: int, survivors: bool) -> float:
+def ref_time_sample(prog, shots: int, seed: int, threads: int, survivors: bool,
+                    omp_threads: int = 1) -> float:
+    """Wall seconds of the reference's clifft::sample (or sample_survivors) over
+    `shots` shots split across `threads` host threads (distinct seeds), each
+    thread's OpenMP team limited to `omp_threads` (the executor parallelises
+    one shot's statevector loops with OpenMP at large k)."""
     lib = ref_lib()
-    t = lib.ref_time_sample(ctypes.byref(prog.image()), shots, seed, threads, int(survivors))
+    t = lib.ref_time_sample_omp(ctypes.byref(prog.image()), shots, seed, threads, int(survivors),
+                                omp_threads)
     if t < 0:
         raise RuntimeError(lib.ref_last_error().decode())
     return t

@@ -27,6 +27,8 @@
 
 #include "clifft_program_image.h"
 
+#include <omp.h>
+
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -459,12 +461,13 @@ int64_t ref_sample_survivors(const clifft_program_image* img, uint32_t shots, ui
 // Wall-clock timing of clifft::sample / sample_survivors on `threads` host
 // threads, each running its own contiguous shot slice with seed `seed + t`
 // (the shot-parallel CPU baseline). Returns elapsed seconds, < 0 on error.
-double ref_time_sample(const clifft_program_image* img, uint64_t shots, uint64_t seed,
-                       int threads, int survivors) {
+double ref_time_sample_omp(const clifft_program_image* img, uint64_t shots, uint64_t seed,
+                           int threads, int survivors, int omp_threads) {
     double secs = -1.0;
     guarded([&] {
         auto m = module_from_image(img);
         if (threads < 1) threads = 1;
+        if (omp_threads < 1) omp_threads = 1;
         std::vector<std::thread> pool;
         std::vector<std::string> errs(threads);
         auto t0 = std::chrono::steady_clock::now();
@@ -472,6 +475,9 @@ double ref_time_sample(const clifft_program_image* img, uint64_t shots, uint64_t
             uint64_t lo = shots * t / threads, hi = shots * (t + 1) / threads;
             pool.emplace_back([&, t, lo, hi] {
                 try {
+                    // OpenMP team size of this worker's own parallel regions
+                    // (the executor's intra-shot loops for large k)
+                    omp_set_num_threads(omp_threads);
                     if (survivors)
                         (void)sample_survivors(*m, static_cast<uint32_t>(hi - lo), seed + t, false);
                     else
@@ -489,6 +495,11 @@ double ref_time_sample(const clifft_program_image* img, uint64_t shots, uint64_t
         return 0;
     });
     return secs;
+}
+
+double ref_time_sample(const clifft_program_image* img, uint64_t shots, uint64_t seed, int threads,
+                       int survivors) {
+    return ref_time_sample_omp(img, shots, seed, threads, survivors, 1);
 }
 
 // Forced replay of `shots` trajectories, executed one instruction at a time.

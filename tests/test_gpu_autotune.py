@@ -29,7 +29,7 @@ def test_autotune_picks_a_candidate_and_matches_fixed_shapes(name):
     first = cb.run(prog, shots, 21, precision="fp64")
     assert first["kernel_launches"] > 1  # trial launches ran
     again = cb.run(prog, shots, 21, precision="fp64")
-    assert again["kernel_launches"] == 1  # cached on the program handle
+    assert again["kernel_launches"] == 1  # cached for this program content
     assert again["group_threads"] == first["group_threads"]
     for r in (first, again):
         assert np.array_equal(r["meas_words"], fixed["meas_words"])
@@ -37,7 +37,15 @@ def test_autotune_picks_a_candidate_and_matches_fixed_shapes(name):
         np.testing.assert_allclose(r["exp_vals"], fixed["exp_vals"], atol=1e-12)
 
 
+def test_tuning_is_shared_by_handles_of_the_same_program():
+    a = _prog("cfg2_12")
+    cb.run(a, 4096, 3, precision="fp32")
+    b = _prog("cfg2_12")  # a second upload of the same content
+    r = cb.run(b, 4096, 3, precision="fp32")
+    assert r["kernel_launches"] == 1
+
+
 def test_small_calls_do_not_tune():
-    prog = _prog("cfg2_12")
+    prog = _prog("cfg2_20")
     r = cb.run(prog, 200, 1, precision="fp32")
     assert r["kernel_launches"] == 1
