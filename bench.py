@@ -3,8 +3,9 @@
 Headline workload (one "step"): `sample` of the k = 24 program (random
 near-Clifford circuit, n = 64, 400 layers, 24 T gates, peak rank 24; bytecode
 after the reference's own bytecode passes, tests/golden/programs/cfg3.npz
-written by tests/golden/make_golden.py) for 296 shots per GPU, i.e. two
-resident waves of one CTA per SM with a 128 MiB complex-FP32 statevector each.
+written by tests/golden/make_golden.py) for 296 shots per GPU, i.e. one
+resident wave of two 256-thread CTAs per SM, each holding a 128 MiB
+complex-FP32 statevector.
 Synthetic seeded data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl clifft_b200|reference]
@@ -38,7 +39,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PROGRAMS = os.path.join(ROOT, "tests", "golden", "programs")
 HEADLINE = "cfg3"
-SHOTS_PER_GPU = 296  # two waves of 148 resident CTAs
+SHOTS_PER_GPU = 296  # one wave of two resident CTAs on each of the 148 SMs
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 METRIC = "shots/sec at k=10/16/24, FP32-batched vs FP64 GPU (1e-5 prob tol); HBM GB/s vs peak"
 WORKLOAD = ("cfg3: random near-Clifford n=64, 400 layers, 24 T, peak k=24 (2^24 amplitudes/shot); "
@@ -114,7 +115,7 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ GPU helpers
-def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False):
+def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False, group=0):
     """One device-resident sampling step: program resident, outputs in HBM.
     plain = the plain executor: one pass per opcode, fixed heuristic launch
     shape (no fusion, no autotuning)."""
@@ -127,7 +128,7 @@ def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=F
         flags |= N.CLIFFT_GPU_NO_FUSION | N.CLIFFT_GPU_NO_AUTOTUNE
     a = N.SampleArgs(shots=shots, seed=seed, first_shot=first_shot,
                      precision=N.CLIFFT_GPU_FP32 if precision == "fp32" else N.CLIFFT_GPU_FP64,
-                     flags=flags, stream=stream.cuda_stream)
+                     flags=flags, group_threads=group, stream=stream.cuda_stream)
     o = N.Outputs()
     for field, t in bufs.items():
         setattr(o, field, t.data_ptr() if t.numel() else None)
@@ -148,7 +149,8 @@ def output_buffers(torch, prog, shots, dev):
     }
 
 
-def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survivors=False, plain=False):
+def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survivors=False, plain=False,
+                group=0):
     import clifft_b200 as cb
     dev = torch.device("cuda", torch.cuda.current_device())
     dp = cb.load(prog)
@@ -156,14 +158,14 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survi
     bufs = output_buffers(torch, prog, shots, dev)
     first = rank * shots
     for w in range(warmup):
-        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain)
+        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain, group)
     torch.cuda.synchronize()
     times, kernel_ms, launches, passed, alg_bytes, streamed, groups = [], [], 0, 0, 0, 0, set()
     for s in range(steps):
         flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain)
+        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain, group)
         ev1.record(stream)
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1))
@@ -330,6 +332,8 @@ def main():
     ap.add_argument("--shots", type=int, default=SHOTS_PER_GPU)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--plain", action="store_true", help="with --profile: the plain executor")
+    ap.add_argument("--group", type=int, default=0,
+                    help="with --profile: fixed group_threads (no autotuning trial launches)")
     args = ap.parse_args()
     if args.profile:
         import torch
@@ -337,7 +341,7 @@ def main():
         prog = load_program(args.profile)
         flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
         r = time_device(torch, prog, args.shots, args.precision, args.steps, args.warmup, 0, flush,
-                        survivors=bool(prog.has_postselection), plain=args.plain)
+                        survivors=bool(prog.has_postselection), plain=args.plain, group=args.group)
         print(json.dumps({"program": args.profile, "shots": args.shots, "precision": args.precision,
                           "plain": args.plain, "ms": r["ms"], "kernel_ms": r["kernel_ms"],
                           "alg_bytes": r["alg_bytes"], "streamed_bytes": r["streamed_bytes"],
@@ -349,7 +353,7 @@ def main():
     config = {"workload": WORKLOAD, "shots_per_gpu_per_step": SHOTS_PER_GPU,
               "global_batch_shots": SHOTS_PER_GPU * world, "peak_k": 24,
               "parallelism": f"shot-sharded x{world}",
-              "l2": "statevectors (128 MiB each, 148 resident) far exceed L2; a 256 MiB buffer is also "
+              "l2": "statevectors (128 MiB each, 296 resident) far exceed L2; a 256 MiB buffer is also "
                     "zeroed between timed steps"}
 
     if args.impl == "reference":
