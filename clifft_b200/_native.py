@@ -82,6 +82,14 @@ def lib():
             L.clifft_gpu_sample.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.POINTER(Outputs)]
             L.clifft_gpu_sample_noalloc.restype = ctypes.c_int
             L.clifft_gpu_sample_noalloc.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.POINTER(Outputs)]
+            L.clifft_gpu_batch_create.restype = ctypes.c_int
+            L.clifft_gpu_batch_create.argtypes = [ctypes.POINTER(P), ctypes.POINTER(SampleArgs),
+                                                  ctypes.POINTER(Outputs), ctypes.c_uint32, ctypes.POINTER(P)]
+            L.clifft_gpu_batch_run.restype = ctypes.c_int
+            L.clifft_gpu_batch_run.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), P,
+                                               ctypes.POINTER(ctypes.c_float)]
+            L.clifft_gpu_batch_free.restype = None
+            L.clifft_gpu_batch_free.argtypes = [P]
             L.clifft_gpu_backend_name.restype = ctypes.c_char_p
             L.clifft_gpu_last_error.restype = ctypes.c_char_p
             L.clifft_gpu_program_peak_rank.restype = ctypes.c_uint32
@@ -95,7 +103,7 @@ def lib():
 EXPORTED_SYMBOLS = (
     "clifft_gpu_load", "clifft_gpu_free", "clifft_gpu_sample", "clifft_gpu_backend_name",
     "clifft_gpu_last_error", "clifft_gpu_program_peak_rank", "clifft_gpu_program_device_bytes",
-    "clifft_gpu_sample_noalloc",
+    "clifft_gpu_sample_noalloc", "clifft_gpu_batch_create", "clifft_gpu_batch_run", "clifft_gpu_batch_free",
 )
 NOALLOC_SCRATCH_WORDS = 512  # CLIFFT_GPU_NOALLOC_SCRATCH_WORDS
 

@@ -403,8 +403,17 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     L.fuse = L.tiles && allow_fusion;
     L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
-    CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(L.smem)));
+    {
+        // only ever raised: launches planned earlier (a captured batch graph,
+        // another host thread) keep a valid limit
+        static std::mutex attr_mu;
+        std::lock_guard<std::mutex> lock(attr_mu);
+        cudaFuncAttributes cur{};
+        CUDA_OK(cudaFuncGetAttributes(&cur, (const void*)L.fn));
+        if (cur.maxDynamicSharedSizeBytes < int(L.smem))
+            CUDA_OK(cudaFuncSetAttribute((const void*)L.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(L.smem)));
+    }
     int per_sm = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)L.fn, L.threads, L.smem));
     if (per_sm < 1) invalid("kernel does not fit on an SM with this launch shape");
@@ -1029,5 +1038,253 @@ int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_
         for (int i = 0; i < 5; ++i) out->phase_cycles[i] = 0;
     });
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------- multi-program batches
+// A batch is an explicitly built CUDA graph with one (memset scratch ->
+// sampling kernel) branch per program and no edges between branches, so one
+// graph launch runs programs of different peak rank side by side, each with
+// its own launch shape (autotuned by the warm-up call at creation).
+struct clifft_gpu_batch {
+    struct Item {
+        clifft_gpu_program* prog = nullptr;
+        clifft_gpu_outputs* out = nullptr;
+        LaunchPlan L{};
+        KParams K{};
+        unsigned long long* scratch = nullptr;  // inside the batch's scratch block
+        size_t scratch_words = 0;
+        size_t scratch_at = 0;                  // word offset in the block
+        void* slab = nullptr;
+        cudaGraphNode_t kernel_node{};
+        void* kargs[2] = {nullptr, nullptr};
+    };
+    std::vector<Item> items;
+    int device = 0;
+    unsigned long long* scratch_block = nullptr;
+    size_t scratch_block_words = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<std::pair<KernelFn, size_t>> smem_limits;
+};
+
+namespace {
+
+void batch_release(clifft_gpu_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    for (auto& it : b->items)
+        if (it.slab) cudaFree(it.slab);
+    if (b->scratch_block) cudaFree(b->scratch_block);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_sample_args* args,
+                            clifft_gpu_outputs* outs, uint32_t n, clifft_gpu_batch** out) {
+    clifft_gpu_batch* b = nullptr;
+    int rc = guarded([&] {
+        if (!progs || !args || !outs || !out || n == 0) invalid("null argument or empty batch");
+        *out = nullptr;
+        b = new clifft_gpu_batch();
+        b->device = progs[0]->device;
+        CUDA_OK(cudaSetDevice(b->device));
+        size_t slab_total = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            clifft_gpu_program* p = progs[i];
+            const clifft_gpu_sample_args& a = args[i];
+            if (!p) invalid("null program in batch");
+            if (p->device != b->device) invalid("all programs of a batch must live on one device");
+            if (!(a.flags & CLIFFT_GPU_DEVICE_PTRS))
+                invalid("batch entries need CLIFFT_GPU_DEVICE_PTRS (outputs stay on the device)");
+            if (a.flags & (CLIFFT_GPU_TRACE | CLIFFT_GPU_PROFILE))
+                invalid("batch entries do not support CLIFFT_GPU_TRACE or CLIFFT_GPU_PROFILE");
+            if (a.shots == 0) invalid("batch entries need at least one shot");
+        }
+        // warm-up call per program: full validation, the autotuned shape, kernel attributes
+        for (uint32_t i = 0; i < n; ++i) {
+            const int r = clifft_gpu_sample(progs[i], &args[i], &outs[i]);
+            if (r != 0) throw ApiError(r, std::string("batch entry ") + std::to_string(i) + ": " + g_last_error);
+        }
+        b->items.resize(n);
+        size_t words = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            auto& it = b->items[i];
+            clifft_gpu_program* p = progs[i];
+            const clifft_gpu_sample_args& a = args[i];
+            const clifft_program_image& m = p->meta;
+            it.prog = p;
+            it.out = &outs[i];
+            const uint32_t rec_words = (m.total_meas_slots + 31) / 32;
+            const uint32_t det_words = (m.num_detectors + 31) / 32;
+            const uint32_t obs_words = (m.num_observables + 31) / 32;
+            const bool allow_fusion = (a.flags & CLIFFT_GPU_NO_FUSION) == 0;
+            uint32_t group_req = a.group_threads;
+            if (group_req == 0 && !(a.flags & CLIFFT_GPU_NO_AUTOTUNE)) {
+                const bool fm = (a.flags & CLIFFT_GPU_FORCED_MEAS) != 0, ff = (a.flags & CLIFFT_GPU_FORCED_FAULTS) != 0;
+                const uint32_t key = a.precision | (allow_fusion ? 2u : 0u) | (a.flags & CLIFFT_GPU_SURVIVORS ? 4u : 0u) |
+                                     (fm ? 8u : 0u) | (ff ? 16u : 0u);
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                auto f = g_tuned.find(std::make_tuple(p->content_hash, p->device, key));
+                if (f != g_tuned.end()) group_req = f->second;
+            }
+            it.L = plan_launch(*p, a.precision, group_req, a.shots, rec_words, det_words, obs_words, allow_fusion);
+            KParams& K = it.K;
+            K.shots = a.shots;
+            K.first_shot = a.first_shot;
+            K.seed = a.seed;
+            K.dust_eps = a.dust_eps > 0.0 ? a.dust_eps : (a.precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
+            K.flags = (a.flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
+                      (a.flags & CLIFFT_GPU_FORCED_MEAS ? KF_FORCED_MEAS : 0) |
+                      (a.flags & CLIFFT_GPU_FORCED_FAULTS ? KF_FORCED_FAULTS : 0) | (it.L.fuse ? KF_FUSE : 0);
+            K.fuse_bytes = it.L.tiles ? (a.precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(it.L.stages)
+                                                                       : fuse_smem_bytes<double>(it.L.stages))
+                                      : 0;
+            K.stages = it.L.stages;
+            K.rec_words = rec_words;
+            K.det_words = det_words;
+            K.obs_words = obs_words;
+            K.meas_out_words = (m.num_measurements + 63) / 64;
+            K.det_out_words = (m.num_detectors + 63) / 64;
+            K.obs_out_words = (m.num_observables + 63) / 64;
+            K.state_in_smem = it.L.state_in_smem ? 1 : 0;
+            K.state_stride = it.L.state_stride;
+            K.forced_meas = (a.flags & CLIFFT_GPU_FORCED_MEAS) ? a.forced_meas : nullptr;
+            if (a.flags & CLIFFT_GPU_FORCED_FAULTS) {
+                K.fault_off = a.fault_offsets;
+                K.ro_off = a.readout_offsets;
+                K.fault_sites = a.fault_sites;
+                K.fault_chan = a.fault_channels;
+                K.ro_entries = a.readout_entries;
+            }
+            K.out_meas = K.meas_out_words ? outs[i].meas : nullptr;
+            K.out_det = K.det_out_words ? outs[i].det : nullptr;
+            K.out_obs = K.obs_out_words ? outs[i].obs : nullptr;
+            K.out_exp = m.num_exp_vals ? outs[i].exp_vals : nullptr;
+            K.out_survived = outs[i].survived;
+            it.scratch_words = 2 + 5 + m.num_observables + 8;
+            it.scratch_at = words;
+            words += (it.scratch_words + 31) & ~size_t(31);
+            if (!it.L.state_in_smem) {
+                const size_t amp = a.precision == CLIFFT_GPU_FP32 ? 8 : 16;
+                const size_t bytes = size_t(it.L.blocks) * it.L.regions * it.L.S * it.L.state_stride * amp;
+                slab_total += bytes;
+                CUDA_OK(cudaMalloc(&it.slab, bytes));
+                K.state_global = it.slab;
+            }
+        }
+        (void)slab_total;
+        CUDA_OK(cudaMalloc(&b->scratch_block, words * 8));
+        b->scratch_block_words = words;
+        CUDA_OK(cudaGraphCreate(&b->graph, 0));
+        for (auto& it : b->items) {
+            it.scratch = b->scratch_block + it.scratch_at;
+            KParams& K = it.K;
+            K.work_counter = it.scratch;
+            K.error_word = reinterpret_cast<int*>(it.scratch + 1);
+            K.counters = it.scratch + 2;
+            K.phase_cycles = nullptr;
+            K.error_info = it.scratch + it.scratch_words - 8;
+            cudaMemsetParams ms{};
+            ms.dst = it.scratch;
+            ms.value = 0;
+            ms.elementSize = 1;
+            ms.width = it.scratch_words * 8;
+            ms.height = 1;
+            ms.pitch = 0;
+            cudaGraphNode_t mnode;
+            CUDA_OK(cudaGraphAddMemsetNode(&mnode, b->graph, nullptr, 0, &ms));
+            it.kargs[0] = &it.prog->dev;
+            it.kargs[1] = &it.K;
+            cudaKernelNodeParams kp{};
+            kp.func = (void*)it.L.fn;
+            kp.gridDim = dim3(it.L.blocks);
+            kp.blockDim = dim3(it.L.threads);
+            kp.sharedMemBytes = (unsigned)it.L.smem;
+            kp.kernelParams = it.kargs;
+            CUDA_OK(cudaGraphAddKernelNode(&it.kernel_node, b->graph, &mnode, 1, &kp));
+            bool seen = false;
+            for (auto& sl : b->smem_limits)
+                if (sl.first == it.L.fn) {
+                    sl.second = std::max(sl.second, it.L.smem);
+                    seen = true;
+                }
+            if (!seen) b->smem_limits.push_back({it.L.fn, it.L.smem});
+        }
+        CUDA_OK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        CUDA_OK(cudaEventCreate(&b->e0));
+        CUDA_OK(cudaEventCreate(&b->e1));
+        *out = b;
+    });
+    if (rc != 0) batch_release(b);
+    return rc;
+}
+
+int clifft_gpu_batch_run(clifft_gpu_batch* b, const uint64_t* seeds, void* stream, float* graph_ms) {
+    return guarded([&] {
+        if (!b) invalid("null batch");
+        CUDA_OK(cudaSetDevice(b->device));
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (seeds) {
+            for (auto& it : b->items) {
+                it.K.seed = seeds[&it - b->items.data()];
+                cudaKernelNodeParams kp{};
+                kp.func = (void*)it.L.fn;
+                kp.gridDim = dim3(it.L.blocks);
+                kp.blockDim = dim3(it.L.threads);
+                kp.sharedMemBytes = (unsigned)it.L.smem;
+                kp.kernelParams = it.kargs;
+                CUDA_OK(cudaGraphExecKernelNodeSetParams(b->exec, it.kernel_node, &kp));
+            }
+        }
+        for (auto& sl : b->smem_limits) {
+            cudaFuncAttributes cur{};
+            CUDA_OK(cudaFuncGetAttributes(&cur, (const void*)sl.first));
+            if (cur.maxDynamicSharedSizeBytes < int(sl.second))
+                CUDA_OK(cudaFuncSetAttribute((const void*)sl.first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(sl.second)));
+        }
+        CUDA_OK(cudaEventRecord(b->e0, st));
+        CUDA_OK(cudaGraphLaunch(b->exec, st));
+        CUDA_OK(cudaEventRecord(b->e1, st));
+        std::vector<unsigned long long> hs(b->scratch_block_words);
+        CUDA_OK(cudaMemcpyAsync(hs.data(), b->scratch_block, hs.size() * 8, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        float ms = 0.f;
+        CUDA_OK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+        if (graph_ms) *graph_ms = ms;
+        for (auto& it : b->items) {
+            const unsigned long long* w = hs.data() + it.scratch_at;
+            const int dev_err = static_cast<int>(w[1] & 0xffffffffu);
+            if (dev_err != 0)
+                throw ApiError(CLIFFT_GPU_EDEVICE, "batch entry " + std::to_string(&it - b->items.data()) +
+                                                       ": device error " + std::to_string(dev_err));
+            clifft_gpu_outputs* o = it.out;
+            o->passed_shots = w[2];
+            o->logical_errors = w[3];
+            o->dust_clamps = w[4];
+            o->algorithmic_bytes = w[5];
+            o->streamed_bytes = w[6];
+            if (o->observable_ones)
+                for (uint32_t j = 0; j < it.prog->meta.num_observables; ++j) o->observable_ones[j] = w[7 + j];
+            o->kernel_launches = 1;
+            o->kernel_ms = ms;
+            o->group_threads = it.L.G ? uint32_t(it.L.G) : uint32_t(it.L.threads);
+            o->state_in_smem = it.L.state_in_smem ? 1u : 0u;
+            o->fused = it.L.fuse ? 1u : 0u;
+        }
+    });
+}
+
+void clifft_gpu_batch_free(clifft_gpu_batch* b) { batch_release(b); }
 
 }  // extern "C"

@@ -183,6 +183,35 @@ const char* clifft_gpu_last_error(void);
 #define CLIFFT_GPU_NOALLOC_SCRATCH_WORDS 512u
 int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
                               clifft_gpu_outputs* out);
+/*
+ * Multi-program batches (the batched form of clifft::sample over many
+ * programs, e.g. a sweep of circuits with different peak rank). A batch is a
+ * CUDA graph with one independent branch per program (clear scratch, sampling
+ * kernel), so a single graph launch runs all programs side by side, each with
+ * its own launch shape.
+ *
+ *   clifft_gpu_batch_create  n programs, n argument blocks and n output blocks.
+ *                            Every entry needs CLIFFT_GPU_DEVICE_PTRS (its inputs
+ *                            and records stay in device buffers the caller keeps
+ *                            alive for the batch's lifetime); TRACE / PROFILE are
+ *                            rejected. Creation runs each entry once through
+ *                            clifft_gpu_sample (validation, autotuning), then
+ *                            allocates the batch's own statevector slabs and
+ *                            scratch and instantiates the graph.
+ *   clifft_gpu_batch_run     replays the graph on `stream` (seeds[i] replaces
+ *                            entry i's seed when `seeds` is non-NULL), waits, and
+ *                            fills each entry's host-side counters (passed_shots,
+ *                            observable_ones, ... of the output blocks given at
+ *                            creation); *graph_ms = device time of the replay.
+ *   clifft_gpu_batch_free    releases the graph, slabs and scratch.
+ *
+ * No counterpart in the reference (its sample() runs one program per call).
+ */
+typedef struct clifft_gpu_batch clifft_gpu_batch;
+int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_sample_args* args,
+                            clifft_gpu_outputs* outs, uint32_t n, clifft_gpu_batch** out);
+int clifft_gpu_batch_run(clifft_gpu_batch* batch, const uint64_t* seeds, void* stream, float* graph_ms);
+void clifft_gpu_batch_free(clifft_gpu_batch* batch);
 /* Program metadata accessors (host memory). */
 uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog);
 uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog);
