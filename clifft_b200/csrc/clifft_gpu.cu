@@ -20,6 +20,7 @@
 
 #include "clifft_gpu.h"
 #include "svm_dispatch.h"
+#include "svm_grad.h"
 #include "svm_kernel.cuh"
 
 using namespace cgpu;
@@ -250,6 +251,8 @@ struct clifft_gpu_program {
     std::vector<uint8_t> expected_host;
     int device = 0;
     uint64_t content_hash = 0;  // FNV-1a of the device image and the launch-relevant counts
+    std::vector<uint8_t> instr_host;  // the 32-byte instructions (host copy, for gradient programs)
+    uint32_t num_rot_params = 0;      // ARRAY_ROT + EXPAND_ROT instructions
     // Statevector slab kept between calls (mapping tens of GB afresh on every
     // call costs more than a large-k launch's own setup). One call at a time
     // holds it; a concurrent call on the same handle allocates its own.
@@ -556,6 +559,12 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
                                        im.num_observables, im.num_exp_vals, im.num_words, im.num_instructions};
             p->content_hash = fnv1a(reinterpret_cast<const uint8_t*>(counts), sizeof(counts),
                                     fnv1a(b.bytes.data(), b.bytes.size()));
+        }
+        p->instr_host.assign(static_cast<const uint8_t*>(im.instructions),
+                             static_cast<const uint8_t*>(im.instructions) + size_t(im.num_instructions) * 32);
+        for (uint32_t i = 0; i < im.num_instructions; ++i) {
+            const uint8_t op = p->instr_host[size_t(i) * 32];
+            if (op == CLIFFT_OP_ARRAY_ROT || op == CLIFFT_OP_EXPAND_ROT) ++p->num_rot_params;
         }
         CUDA_OK(cudaMalloc(&p->blob, b.bytes.size()));
         p->blob_bytes = b.bytes.size();
@@ -1286,5 +1295,146 @@ int clifft_gpu_batch_run(clifft_gpu_batch* b, const uint64_t* seeds, void* strea
 }
 
 void clifft_gpu_batch_free(clifft_gpu_batch* b) { batch_release(b); }
+
+}  // extern "C"
+
+// ------------------------------------------------- expectation-value gradients
+namespace {
+
+
+const char* opcode_name(uint32_t op) {
+    static const char* names[] = {
+        "FRAME_CNOT", "FRAME_CZ", "FRAME_H", "FRAME_S", "FRAME_S_DAG", "FRAME_SWAP", "ARRAY_CNOT", "ARRAY_CZ",
+        "ARRAY_SWAP", "ARRAY_MULTI_CNOT", "ARRAY_MULTI_CZ", "ARRAY_H", "ARRAY_S", "ARRAY_S_DAG", "ARRAY_T",
+        "ARRAY_T_DAG", "ARRAY_ROT", "ARRAY_U2", "ARRAY_U4", "EXPAND", "EXPAND_T", "EXPAND_T_DAG", "EXPAND_ROT"};
+    return op < sizeof(names) / sizeof(names[0]) ? names[op] : "a measurement / noise / classical opcode";
+}
+
+bool grad_supported(uint32_t op) {
+    switch (op) {
+        case CLIFFT_OP_FRAME_CNOT:
+        case CLIFFT_OP_FRAME_CZ:
+        case CLIFFT_OP_FRAME_H:
+        case CLIFFT_OP_FRAME_S:
+        case CLIFFT_OP_FRAME_S_DAG:
+        case CLIFFT_OP_FRAME_SWAP:
+        case CLIFFT_OP_ARRAY_CNOT:
+        case CLIFFT_OP_ARRAY_CZ:
+        case CLIFFT_OP_ARRAY_SWAP:
+        case CLIFFT_OP_ARRAY_MULTI_CNOT:
+        case CLIFFT_OP_ARRAY_MULTI_CZ:
+        case CLIFFT_OP_ARRAY_H:
+        case CLIFFT_OP_ARRAY_S:
+        case CLIFFT_OP_ARRAY_S_DAG:
+        case CLIFFT_OP_ARRAY_T:
+        case CLIFFT_OP_ARRAY_T_DAG:
+        case CLIFFT_OP_ARRAY_ROT:
+        case CLIFFT_OP_EXPAND:
+        case CLIFFT_OP_EXPAND_T:
+        case CLIFFT_OP_EXPAND_T_DAG:
+        case CLIFFT_OP_EXPAND_ROT:
+        case CLIFFT_OP_EXP_VAL: return true;
+        default: return false;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t clifft_gpu_program_num_rot_params(const clifft_gpu_program* prog) {
+    return prog ? prog->num_rot_params : 0;
+}
+
+int clifft_gpu_expval_grad(clifft_gpu_program* prog, const clifft_gpu_grad_args* args, double* exp_vals,
+                           double* grads) {
+    return guarded([&] {
+        if (!prog || !args || !exp_vals) invalid("null argument");
+        const clifft_program_image& m = prog->meta;
+        if (args->precision != CLIFFT_GPU_FP32 && args->precision != CLIFFT_GPU_FP64)
+            invalid("precision must be CLIFFT_GPU_FP32 or CLIFFT_GPU_FP64");
+        const bool dev_ptrs = (args->flags & CLIFFT_GPU_DEVICE_PTRS) != 0;
+        // the program: measurement-free, noise-free, rotations as ARRAY_ROT / EXPAND_ROT
+        const uint32_t n = m.num_instructions;
+        std::vector<int32_t> rot_index(n, -1);
+        std::vector<uint32_t> exp_pc, exp_out;
+        std::vector<uint8_t> seen_out(m.num_exp_vals, 0);
+        uint32_t np = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint8_t* ins = prog->instr_host.data() + size_t(i) * 32;
+            const uint32_t op = ins[0];
+            if (!grad_supported(op)) {
+                std::string why = (op == CLIFFT_OP_ARRAY_U2 || op == CLIFFT_OP_ARRAY_U4)
+                                      ? " (fused U2 / U4 nodes hide the rotation angles: compile gradient "
+                                        "programs without the single-axis / tile-axis fusion passes)"
+                                      : "";
+                invalid("clifft_gpu_expval_grad needs a measurement-free, noise-free program: instruction " +
+                        std::to_string(i) + " is " + opcode_name(op) + why);
+            }
+            if (op == CLIFFT_OP_ARRAY_ROT || op == CLIFFT_OP_EXPAND_ROT) rot_index[i] = int32_t(np++);
+            if (op == CLIFFT_OP_EXP_VAL) {
+                uint32_t out_idx = 0;
+                std::memcpy(&out_idx, ins + 12, 4);
+                if (out_idx >= m.num_exp_vals || seen_out[out_idx]) invalid("EXP_VAL output rows must be distinct");
+                seen_out[out_idx] = 1;
+                exp_pc.push_back(i);
+                exp_out.push_back(out_idx);
+            }
+        }
+        if (np != prog->num_rot_params) invalid("internal: rotation count mismatch");
+        const uint64_t batch = args->batch;
+        if (batch == 0 || exp_pc.empty()) return;
+        if (np > 0 && !grads) invalid("grads output is null");
+        CUDA_OK(cudaSetDevice(prog->device));
+        cudaStream_t st = static_cast<cudaStream_t>(args->stream);
+        StreamBuffers buf(st);
+        auto up = [&](const void* src, size_t bytes) -> void* {
+            void* d = buf.alloc(bytes);
+            if (d) CUDA_OK(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st));
+            return d;
+        };
+        GradParams G{};
+        G.batch = batch;
+        G.n_exp = uint32_t(exp_pc.size());
+        G.n_out = m.num_exp_vals;
+        G.n_params = np;
+        G.rot_index = static_cast<const int32_t*>(up(rot_index.data(), rot_index.size() * 4));
+        G.exp_pc = static_cast<const uint32_t*>(up(exp_pc.data(), exp_pc.size() * 4));
+        G.exp_out = static_cast<const uint32_t*>(up(exp_out.data(), exp_out.size() * 4));
+        if (args->phases && np) {
+            G.phases = dev_ptrs ? args->phases
+                                : static_cast<const double*>(up(args->phases, size_t(batch) * np * 8));
+        }
+        const size_t out_e = size_t(batch) * m.num_exp_vals * 8, out_g = size_t(batch) * m.num_exp_vals * np * 8;
+        G.out_exp = dev_ptrs ? exp_vals : static_cast<double*>(buf.alloc(out_e));
+        G.out_grad = dev_ptrs ? grads : static_cast<double*>(buf.alloc(std::max<size_t>(out_g, 8)));
+        // rows of EXP_VAL outputs no instruction writes stay zero
+        CUDA_OK(cudaMemsetAsync(G.out_exp, 0, out_e, st));
+        if (out_g) CUDA_OK(cudaMemsetAsync(G.out_grad, 0, out_g, st));
+        const bool fp32 = args->precision == CLIFFT_GPU_FP32;
+        ExpvalGradFn fn = expval_grad_kernel_fn(fp32);
+        int per_sm = 0, sms = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, kExpvalGradThreads, 0));
+        CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, prog->device));
+        const uint64_t tasks = batch * G.n_exp;
+        G.stride = uint64_t(1) << m.peak_rank;
+        const size_t amp = fp32 ? 8 : 16;
+        size_t free_b = 0, total_b = 0;
+        CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
+        uint64_t blocks = std::min<uint64_t>(tasks, uint64_t(std::max(per_sm, 1)) * sms);
+        blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, (free_b / 2) / (2 * G.stride * amp)));
+        G.slab = buf.alloc(size_t(blocks) * 2 * G.stride * amp);
+        auto* work = static_cast<unsigned long long*>(buf.alloc(64));
+        CUDA_OK(cudaMemsetAsync(work, 0, 64, st));
+        G.work = work;
+        fn<<<unsigned(blocks), kExpvalGradThreads, 0, st>>>(prog->dev, G);
+        CUDA_OK(cudaGetLastError());
+        if (!dev_ptrs) {
+            CUDA_OK(cudaMemcpyAsync(exp_vals, G.out_exp, out_e, cudaMemcpyDeviceToHost, st));
+            if (out_g) CUDA_OK(cudaMemcpyAsync(grads, G.out_grad, out_g, cudaMemcpyDeviceToHost, st));
+        }
+        CUDA_OK(cudaStreamSynchronize(st));
+    });
+}
 
 }  // extern "C"

@@ -650,3 +650,31 @@ def config4(seed: int = 3, n: int = 40, layers: int = 120, n_rot: int = 32,
         letters = "".join("XYZ"[int(v)] for v in prng.integers(0, 3, size=4))
         c.add("EXPVAL", *[int(q) for q in qs], pauli=letters)
     return c, theta[np.array(order, dtype=np.int64)]
+
+
+def active_probes(program, seed: int = 0):
+    """`program` with every EXP_VAL mask redrawn as a low-weight Pauli (X / Y
+    on one or two axes, Z on up to two) on the axes active at that
+    instruction, in the compiled frame basis. Random weight-4 probes in the
+    circuit basis of a scrambled Clifford circuit read 0, and so do their
+    derivatives (their X / Y support lands on dormant axes); these probes have
+    non-trivial values and slopes, so gradient checks and timings exercise the
+    whole backward pass."""
+    import numpy as np
+    from .program import OP, Program
+    rng = np.random.default_rng(seed)
+    hist = program.active_k_history()
+    ex, ez, es = program.exp_val_x.copy(), program.exp_val_z.copy(), program.exp_val_sign.copy()
+    for pc in np.nonzero(program.opcodes == OP["EXP_VAL"])[0]:
+        cp = int(program.instructions[pc, 8:12].copy().view(np.uint32)[0])
+        k = int(hist[pc])
+        xs = rng.choice(k, size=int(rng.integers(1, 3)), replace=False)
+        zs = rng.choice(k, size=int(rng.integers(0, 3)), replace=False)
+        ex[cp] = 0
+        ez[cp] = 0
+        ex[cp, 0] = np.uint64(sum(1 << int(a) for a in xs))
+        ez[cp, 0] = np.uint64(sum(1 << int(a) for a in zs))
+        es[cp] = rng.integers(0, 2)
+    d = program.to_npz_dict()
+    d["exp_val_x"], d["exp_val_z"], d["exp_val_sign"] = ex, ez, es
+    return Program.from_npz_dict(d)

@@ -212,6 +212,35 @@ int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_s
                             clifft_gpu_outputs* outs, uint32_t n, clifft_gpu_batch** out);
 int clifft_gpu_batch_run(clifft_gpu_batch* batch, const uint64_t* seeds, void* stream, float* graph_ms);
 void clifft_gpu_batch_free(clifft_gpu_batch* batch);
+/*
+ * Gradients of expectation values by the adjoint method (d<P>/dtheta for
+ * every continuous rotation of a measurement-free, noise-free program). No
+ * counterpart in the reference, which has no differentiation.
+ *
+ * Parameters are the rotation instructions (ARRAY_ROT and EXPAND_ROT) in
+ * program order, clifft_gpu_program_num_rot_params of them; parameter j is the
+ * phase angle phi_j (radians) of its payload (cos phi, sin phi), the phase the
+ * executor puts on the |1> half of the rotated axis. For each of `batch`
+ * parameter vectors (args->phases, batch x num_rot_params, or NULL to use the
+ * program's own payloads for every row) the call returns every EXP_VAL row
+ * (exp_vals, batch x num_exp_vals) and its derivatives (grads, batch x
+ * num_exp_vals x num_rot_params). The kernel runs each (vector, EXP_VAL) pair
+ * forward to the EXP_VAL, then back through the bytecode, undoing each
+ * instruction with its inverse (no per-instruction state is stored) and
+ * accumulating the derivatives in FP64; args->precision selects the
+ * statevector precision. Programs with measurements, noise, classical records
+ * or fused U2 / U4 nodes are rejected (CLIFFT_GPU_EINVAL).
+ */
+typedef struct clifft_gpu_grad_args {
+    uint64_t batch;        /* parameter vectors */
+    uint32_t precision;    /* CLIFFT_GPU_FP64 or CLIFFT_GPU_FP32 statevector */
+    uint32_t flags;        /* CLIFFT_GPU_DEVICE_PTRS: phases, exp_vals and grads are device pointers */
+    const double* phases;  /* batch x num_rot_params, or NULL */
+    void* stream;          /* cudaStream_t; NULL = the legacy default stream */
+} clifft_gpu_grad_args;
+uint32_t clifft_gpu_program_num_rot_params(const clifft_gpu_program* prog);
+int clifft_gpu_expval_grad(clifft_gpu_program* prog, const clifft_gpu_grad_args* args, double* exp_vals,
+                           double* grads);
 /* Program metadata accessors (host memory). */
 uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog);
 uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog);

@@ -19,7 +19,8 @@ from clifft_b200.program import (FLAG_EXPECTED_ONE, FLAG_IDENTITY, FLAG_SIGN, OP
 
 def random_program(seed: int, n: int = 10, length: int = 160, max_k: int = 6,
                    noise: bool = True, classical: bool = True, expvals: bool = True,
-                   postselect: bool = False, readout: bool = True, expand_bias: float = 0.12) -> Program:
+                   postselect: bool = False, readout: bool = True, expand_bias: float = 0.12,
+                   measure: bool = True, active_expvals: bool = False) -> Program:
     rng = np.random.default_rng(seed)
     W = (n + 63) // 64
     k = 0
@@ -124,7 +125,7 @@ def random_program(seed: int, n: int = 10, length: int = 160, max_k: int = 6,
                 emit(OP["ARRAY_ROT"], a, payload=p_f64x2(math.cos(t * math.pi), math.sin(t * math.pi)))
             else:
                 emit(OP["ARRAY_T"] if c == 0 else OP["ARRAY_T_DAG"], a)
-        elif r < 0.74:
+        elif r < 0.74 and measure:
             # measurement
             sign = FLAG_SIGN if rng.random() < 0.3 else 0
             c = rng.integers(0, 5)
@@ -181,6 +182,8 @@ def random_program(seed: int, n: int = 10, length: int = 160, max_k: int = 6,
                 nobs = max(nobs, 2)
         elif r < 0.90 and expvals:
             x, z = rmask()
+            if active_expvals:
+                x &= (1 << k) - 1  # X / Y only on active axes: a non-zero expectation
             expm.append((x, z, int(rng.integers(0, 2))))
             emit(OP["EXP_VAL"], payload=p_u32x2(len(expm) - 1, nexp))
             nexp += 1
