@@ -97,6 +97,8 @@ def lib():
                                                ctypes.POINTER(ctypes.c_float)]
             L.clifft_gpu_batch_free.restype = None
             L.clifft_gpu_batch_free.argtypes = [P]
+            L.clifft_gpu_sample_k.restype = ctypes.c_int
+            L.clifft_gpu_sample_k.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.c_uint32, ctypes.POINTER(Outputs)]
             L.clifft_gpu_expval_grad.restype = ctypes.c_int
             L.clifft_gpu_expval_grad.argtypes = [P, ctypes.POINTER(GradArgs), P, P]
             L.clifft_gpu_program_num_rot_params.restype = ctypes.c_uint32
@@ -115,7 +117,7 @@ EXPORTED_SYMBOLS = (
     "clifft_gpu_load", "clifft_gpu_free", "clifft_gpu_sample", "clifft_gpu_backend_name",
     "clifft_gpu_last_error", "clifft_gpu_program_peak_rank", "clifft_gpu_program_device_bytes",
     "clifft_gpu_sample_noalloc", "clifft_gpu_batch_create", "clifft_gpu_batch_run", "clifft_gpu_batch_free",
-    "clifft_gpu_expval_grad", "clifft_gpu_program_num_rot_params",
+    "clifft_gpu_expval_grad", "clifft_gpu_program_num_rot_params", "clifft_gpu_sample_k",
 )
 NOALLOC_SCRATCH_WORDS = 512  # CLIFFT_GPU_NOALLOC_SCRATCH_WORDS
 

@@ -87,13 +87,15 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
-        profile: bool = False, autotune: bool = True) -> Dict[str, object]:
+        profile: bool = False, autotune: bool = True, k_faults: Optional[int] = None) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None / True = runs of
     consecutive opcodes share one pass over a global-memory statevector,
     False = one pass per opcode (the plain executor). `autotune`: with
     group_threads == 0, let the library time candidate launch shapes on the
-    first large call and keep the fastest (False = fixed heuristic)."""
+    first large call and keep the fastest (False = fixed heuristic).
+    `k_faults`: condition every shot on exactly that many fault events
+    (clifft_gpu_sample_k)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:
@@ -162,8 +164,14 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
             setattr(o, field, arr.ctypes.data)
     ones = np.zeros(max(1, p.num_observables), np.uint64)
     o.observable_ones = ones.ctypes.data
-    N.check(N.lib().clifft_gpu_sample(dp.handle, ctypes.byref(a), ctypes.byref(o)),
-            "clifft_gpu_sample")
+    if k_faults is None:
+        N.check(N.lib().clifft_gpu_sample(dp.handle, ctypes.byref(a), ctypes.byref(o)),
+                "clifft_gpu_sample")
+    else:
+        if k_faults < 0:
+            raise ValueError("k must be non-negative")
+        N.check(N.lib().clifft_gpu_sample_k(dp.handle, ctypes.byref(a), int(k_faults), ctypes.byref(o)),
+                "clifft_gpu_sample_k")
     if "final_v" in res:
         fv = res["final_v"]
         res["final_v"] = fv[..., 0] + 1j * fv[..., 1]
@@ -204,7 +212,10 @@ def sample_survivors(program: Program, shots: int, seed: Optional[int] = None,
     Rows are the surviving shots in shot order."""
     r = run(program, shots, seed, precision=precision, survivors=True,
             group_threads=group_threads, want_records=keep_records)
-    p = program
+    return _survivor_result(program, r, keep_records, shots)
+
+
+def _survivor_result(p: Program, r: Dict[str, object], keep_records: bool, shots: int) -> SampleResult:
     if keep_records:
         keep = r["survived"].astype(bool)
         meas = _unpack(r["meas_words"][keep], p.num_measurements)
@@ -254,3 +265,34 @@ def record_probabilities(program: Program, records: np.ndarray, *,
     out = r["log_prob"].copy()
     out[r["survived"] == 0] = np.finfo(np.float64).min
     return out
+
+
+def noise_site_probabilities(program: Program) -> np.ndarray:
+    """Per fault site its total probability: the noise sites (sum of their
+    channel probabilities), then the readout entries
+    (clifft::noise_site_probabilities, src/clifft/svm/svm.cc:356-369)."""
+    p = program
+    off = p.noise_site_offsets.astype(np.int64)
+    sites = [float(sum(p.noise_channel_prob[off[i]:off[i + 1]].tolist())) for i in range(len(off) - 1)]
+    return np.array(sites + [float(x) for x in p.readout_prob], np.float64)
+
+
+def sample_k(program: Program, shots: int, k: int, seed: Optional[int] = None, *,
+             precision: str = "fp32", group_threads: int = 0) -> SampleResult:
+    """clifft.sample_k (src/clifft/svm/svm.cc:548-613): every shot conditioned
+    on exactly k fault events."""
+    r = run(program, shots, seed, precision=precision, group_threads=group_threads, k_faults=k)
+    return SampleResult(_unpack(r["meas_words"], program.num_measurements),
+                        _unpack(r["det_words"], program.num_detectors),
+                        _unpack(r["obs_words"], program.num_observables),
+                        exp_vals=r["exp_vals"], stats=_stats(r))
+
+
+def sample_k_survivors(program: Program, shots: int, k: int, seed: Optional[int] = None,
+                       keep_records: bool = False, *, precision: str = "fp32",
+                       group_threads: int = 0) -> SampleResult:
+    """clifft.sample_k_survivors (src/clifft/svm/svm.cc:615-711). Rows are the
+    surviving shots in shot order."""
+    r = run(program, shots, seed, precision=precision, survivors=True, group_threads=group_threads,
+            want_records=keep_records, k_faults=k)
+    return _survivor_result(program, r, keep_records, shots)

@@ -19,8 +19,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libclifft_gpu.so")
 
-SOURCES = ["clifft_gpu.cu", "svm_kernels_f32.cu", "svm_kernels_f64.cu", "svm_grad.cu"]
-HEADERS = ["svm_kernel.cuh", "svm_dispatch.h", "svm_instantiate.cuh", "svm_grad.h"]
+SOURCES = ["clifft_gpu.cu", "svm_kernels_f32.cu", "svm_kernels_f64.cu", "svm_grad.cu", "svm_sample_k.cu"]
+HEADERS = ["svm_kernel.cuh", "svm_dispatch.h", "svm_instantiate.cuh", "svm_grad.h", "svm_sample_k.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

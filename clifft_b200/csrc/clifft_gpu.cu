@@ -22,6 +22,7 @@
 #include "svm_dispatch.h"
 #include "svm_grad.h"
 #include "svm_kernel.cuh"
+#include "svm_sample_k.h"
 
 using namespace cgpu;
 
@@ -253,6 +254,8 @@ struct clifft_gpu_program {
     uint64_t content_hash = 0;  // FNV-1a of the device image and the launch-relevant counts
     std::vector<uint8_t> instr_host;  // the 32-byte instructions (host copy, for gradient programs)
     uint32_t num_rot_params = 0;      // ARRAY_ROT + EXPAND_ROT instructions
+    std::vector<double> fault_probs;  // per noise site its total probability, then per readout entry its flip
+                                      // probability (clifft::noise_site_probabilities order)
     // Statevector slab kept between calls (mapping tens of GB afresh on every
     // call costs more than a large-k launch's own setup). One call at a time
     // holds it; a concurrent call on the same handle allocates its own.
@@ -560,6 +563,8 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
             p->content_hash = fnv1a(reinterpret_cast<const uint8_t*>(counts), sizeof(counts),
                                     fnv1a(b.bytes.data(), b.bytes.size()));
         }
+        p->fault_probs.assign(psum.begin(), psum.end());
+        for (uint32_t r = 0; r < im.num_readout_noise; ++r) p->fault_probs.push_back(im.readout_prob[r]);
         p->instr_host.assign(static_cast<const uint8_t*>(im.instructions),
                              static_cast<const uint8_t*>(im.instructions) + size_t(im.num_instructions) * 32);
         for (uint32_t i = 0; i < im.num_instructions; ++i) {
@@ -630,8 +635,22 @@ void clifft_gpu_free(clifft_gpu_program* prog) {
 uint32_t clifft_gpu_program_peak_rank(const clifft_gpu_program* prog) { return prog ? prog->meta.peak_rank : 0; }
 uint64_t clifft_gpu_program_device_bytes(const clifft_gpu_program* prog) { return prog ? prog->blob_bytes : 0; }
 
-int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, clifft_gpu_outputs* out) {
-    return guarded([&] {
+}  // extern "C"
+
+namespace {
+
+// Device-resident per-shot fault lists prepared by the library itself
+// (sample_k): begin offsets in args->fault_offsets / readout_offsets, end
+// offsets here, every array a device pointer whatever args->flags says.
+struct DeviceFaults {
+    const uint32_t* fault_end = nullptr;
+    const uint32_t* ro_end = nullptr;
+};
+
+// clifft_gpu_sample; `dfaults` non-null when the forced-fault lists live on
+// the device (the outputs follow args->flags as usual).
+void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, clifft_gpu_outputs* out,
+                 const DeviceFaults* dfaults) {
         if (!prog || !args || !out) invalid("null argument");
         const clifft_program_image& m = prog->meta;
         const uint64_t shots = args->shots;
@@ -662,7 +681,7 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
 
         // host-side validation of forced-fault inputs (bounds only)
         std::vector<uint32_t> h_foff, h_roff;
-        if (forced_faults && !dev_ptrs) {
+        if (forced_faults && !dev_ptrs && !dfaults) {
             for (uint64_t s = 0; s < shots; ++s) {
                 if (args->fault_offsets[s] > args->fault_offsets[s + 1] ||
                     args->readout_offsets[s] > args->readout_offsets[s + 1])
@@ -745,7 +764,15 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         };
         if (forced_meas)
             K.forced_meas = static_cast<const uint8_t*>(stage_in(args->forced_meas, shots * m.total_meas_slots));
-        if (forced_faults) {
+        if (forced_faults && dfaults) {
+            K.fault_off = args->fault_offsets;
+            K.ro_off = args->readout_offsets;
+            K.fault_end = dfaults->fault_end;
+            K.ro_end = dfaults->ro_end;
+            K.fault_sites = args->fault_sites;
+            K.fault_chan = args->fault_channels;
+            K.ro_entries = args->readout_entries;
+        } else if (forced_faults) {
             uint64_t nf = dev_ptrs ? 0 : args->fault_offsets[shots];
             uint64_t nr = dev_ptrs ? 0 : args->readout_offsets[shots];
             K.fault_off = static_cast<const uint32_t*>(stage_in(args->fault_offsets, (shots + 1) * 4));
@@ -896,7 +923,14 @@ int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* ar
         out->state_in_smem = L.state_in_smem ? 1u : 0u;
         out->fused = L.fuse ? 1u : 0u;
         for (int i = 0; i < 5; ++i) out->phase_cycles[i] = profile ? hs[2 + n_counters + i] : 0;
-    });
+}
+
+}  // namespace
+
+extern "C" {
+
+int clifft_gpu_sample(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, clifft_gpu_outputs* out) {
+    return guarded([&] { sample_impl(prog, args, out, nullptr); });
 }
 
 }  // extern "C"
@@ -1434,6 +1468,108 @@ int clifft_gpu_expval_grad(clifft_gpu_program* prog, const clifft_gpu_grad_args*
             if (out_g) CUDA_OK(cudaMemcpyAsync(grads, G.out_grad, out_g, cudaMemcpyDeviceToHost, st));
         }
         CUDA_OK(cudaStreamSynchronize(st));
+    });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ k-fault importance sampling
+extern "C" {
+
+int clifft_gpu_sample_k(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, uint32_t k,
+                        clifft_gpu_outputs* out) {
+    return guarded([&] {
+        if (!prog || !args || !out) invalid("null argument");
+        if (args->flags & (CLIFFT_GPU_FORCED_MEAS | CLIFFT_GPU_FORCED_FAULTS))
+            invalid("clifft_gpu_sample_k draws its own fault sets: forced outcomes / faults are not accepted");
+        // the stratum must carry probability mass (src/clifft/svm/svm.cc:522-545)
+        const std::vector<double>& probs = prog->fault_probs;
+        const uint32_t n_total = uint32_t(probs.size());
+        if (k > n_total)
+            invalid("k (" + std::to_string(k) + ") exceeds total fault sites (" + std::to_string(n_total) + ")");
+        uint32_t n_certain = 0, n_impossible = 0;
+        for (double p : probs) {
+            if (p <= 0.0)
+                n_impossible++;
+            else if (p >= 1.0)
+                n_certain++;
+        }
+        if (k < n_certain || k > n_total - n_impossible)
+            invalid("k-fault stratum k=" + std::to_string(k) + " has zero probability mass (" +
+                    std::to_string(n_certain) + " sites have p=1, " + std::to_string(n_impossible) +
+                    " sites have p=0)");
+        const uint64_t shots = args->shots;
+        if (shots == 0) {
+            sample_impl(prog, args, out, nullptr);
+            return;
+        }
+        const uint64_t stride = std::max<uint32_t>(k, 1);
+        if (shots * stride > 0xffffffffull) invalid("shots x k exceeds 2^32 fault slots; split the call");
+        // sampler tables: equal probabilities -> uniform k-subsets; else odds
+        // ratios (scaled to mean 1) and the suffix subset-weight DP
+        bool uniform = k <= kSampleKUniformMax;
+        for (uint32_t i = 1; i < n_total && uniform; ++i) uniform = probs[i] == probs[0];
+        std::vector<double> w, dp;
+        if (!uniform) {
+            w.resize(n_total);
+            double sum_w = 0.0;
+            for (uint32_t i = 0; i < n_total; ++i) {
+                const double p = std::min(std::max(probs[i], 0.0), 1.0 - 1e-15);
+                w[i] = p / (1.0 - p);
+                sum_w += w[i];
+            }
+            if (sum_w > 0.0)
+                for (double& x : w) x *= double(n_total) / sum_w;
+            const uint32_t st = k + 1;
+            dp.assign(size_t(n_total + 1) * st, 0.0);
+            for (uint32_t i = 0; i <= n_total; ++i) dp[size_t(i) * st] = 1.0;
+            for (int i = int(n_total) - 1; i >= 0; --i) {
+                const uint32_t mx = std::min(n_total - uint32_t(i), k);
+                for (uint32_t j = 1; j <= mx; ++j)
+                    dp[size_t(i) * st + j] = dp[size_t(i + 1) * st + j] + w[i] * dp[size_t(i + 1) * st + (j - 1)];
+            }
+        }
+        CUDA_OK(cudaSetDevice(prog->device));
+        cudaStream_t st = static_cast<cudaStream_t>(args->stream);
+        StreamBuffers buf(st);
+        SampleKParams S{};
+        S.shots = shots;
+        S.first_shot = args->first_shot;
+        S.seed = args->seed;
+        S.k = k;
+        S.n_total = n_total;
+        S.n_q = prog->meta.num_noise_sites;
+        S.uniform = uniform ? 1u : 0u;
+        auto up = [&](const std::vector<double>& v) -> const double* {
+            if (v.empty()) return nullptr;
+            void* d = buf.alloc(v.size() * 8);
+            CUDA_OK(cudaMemcpyAsync(d, v.data(), v.size() * 8, cudaMemcpyHostToDevice, st));
+            return static_cast<const double*>(d);
+        };
+        S.w = up(w);
+        S.dp = up(dp);
+        auto u32 = [&](size_t n) { return static_cast<uint32_t*>(buf.alloc(n * 4)); };
+        S.fault_off = u32(shots);
+        S.fault_end = u32(shots);
+        S.ro_off = u32(shots);
+        S.ro_end = u32(shots);
+        S.fault_sites = u32(shots * stride);
+        S.fault_chan = u32(shots * stride);
+        S.ro_entries = u32(shots * stride);
+        launch_sample_k_prepare(prog->dev, S, st);
+        CUDA_OK(cudaGetLastError());
+        clifft_gpu_sample_args a = *args;
+        a.flags |= CLIFFT_GPU_FORCED_FAULTS;
+        a.fault_offsets = S.fault_off;
+        a.fault_sites = S.fault_sites;
+        a.fault_channels = S.fault_chan;
+        a.readout_offsets = S.ro_off;
+        a.readout_entries = S.ro_entries;
+        DeviceFaults df;
+        df.fault_end = S.fault_end;
+        df.ro_end = S.ro_end;
+        sample_impl(prog, &a, out, &df);
+        out->kernel_launches += 1;
     });
 }
 

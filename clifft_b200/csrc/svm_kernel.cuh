@@ -107,6 +107,8 @@ struct KParams {
     const uint32_t* fault_chan;
     const uint32_t* ro_off;
     const uint32_t* ro_entries;
+    const uint32_t* fault_end;  // optional per-shot end offsets (else fault_off[shot + 1])
+    const uint32_t* ro_end;     // optional per-shot end offsets (else ro_off[shot + 1])
     // outputs
     uint64_t* out_meas;
     uint64_t* out_det;
@@ -222,11 +224,13 @@ __device__ __forceinline__ double2 dmul(double2 a, double2 b) {
 
 // ---------------------------------------------------------------- philox
 // Philox4x32-10 (Salmon et al., SC'11). Draw d of shot s uses counter
-// (d >> 1, 0, s_lo, s_hi) and key (seed_lo, seed_hi); even draws take words
-// (0, 1), odd draws words (2, 3); 53 high bits -> [0, 1) as the reference's
-// random_double (src/clifft/svm/svm.h:150).
-__device__ __forceinline__ double philox_uniform(uint64_t seed, uint64_t shot, uint32_t draw) {
-    uint32_t c0 = draw >> 1, c1 = 0u, c2 = (uint32_t)shot, c3 = (uint32_t)(shot >> 32);
+// (d >> 1, stream, s_lo, s_hi) and key (seed_lo, seed_hi); even draws take
+// words (0, 1), odd draws words (2, 3); 53 high bits -> [0, 1) as the
+// reference's random_double (src/clifft/svm/svm.h:150). Stream 0 feeds the
+// executor; stream 1 the per-shot fault-site draws of sample_k.
+__device__ __forceinline__ double philox_uniform(uint64_t seed, uint64_t shot, uint32_t draw,
+                                                 uint32_t stream = 0u) {
+    uint32_t c0 = draw >> 1, c1 = stream, c2 = (uint32_t)shot, c3 = (uint32_t)(shot >> 32);
     uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
@@ -1980,9 +1984,9 @@ struct Shot {
         if (Grp::rank() == 0) A(0) = Cx<R>::make(1.0, 0.0);
         if (K.flags & KF_FORCED_FAULTS) {
             ff_pos = K.fault_off[shot];
-            ff_end = K.fault_off[shot + 1];
+            ff_end = K.fault_end ? K.fault_end[shot] : K.fault_off[shot + 1];
             ro_pos = K.ro_off[shot];
-            ro_end = K.ro_off[shot + 1];
+            ro_end = K.ro_end ? K.ro_end[shot] : K.ro_off[shot + 1];
             if (ff_pos < ff_end)
                 next_noise = K.fault_sites[ff_pos++];
             else

@@ -184,6 +184,22 @@ const char* clifft_gpu_last_error(void);
 int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_args* args,
                               clifft_gpu_outputs* out);
 /*
+ * k-fault importance sampling: clifft::sample_k / sample_k_survivors
+ * (src/clifft/svm/svm.h:366-372, src/clifft/svm/svm.cc:356-711). Every shot
+ * is conditioned on exactly k fault events among the noise sites and readout
+ * entries (clifft::noise_site_probabilities order: sites, then readout
+ * entries), drawn on the device per shot from the exact conditional
+ * Poisson-binomial distribution (uniform k-subsets when every probability is
+ * equal); a fired site's channel is drawn as the NOISE opcode draws it. Same
+ * arguments and outputs as clifft_gpu_sample (CLIFFT_GPU_SURVIVORS selects
+ * sample_k_survivors); forced outcomes / faults are rejected. Strata without
+ * probability mass are rejected with the reference's messages. The draws use
+ * Philox stream 1 of each shot's counter space, the executor stream 0.
+ */
+int clifft_gpu_sample_k(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, uint32_t k,
+                        clifft_gpu_outputs* out);
+
+/*
  * Multi-program batches (the batched form of clifft::sample over many
  * programs, e.g. a sweep of circuits with different peak rank). A batch is a
  * CUDA graph with one independent branch per program (clear scratch, sampling

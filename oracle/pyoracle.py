@@ -87,6 +87,10 @@ def ref_lib():
         lib.ref_svm_backend.restype = ctypes.c_char_p
         lib.ref_sample.restype = ctypes.c_int
         lib.ref_sample.argtypes = [P, ctypes.c_uint32, ctypes.c_uint64, P, P, P, P]
+        lib.ref_sample_k.restype = ctypes.c_int
+        lib.ref_sample_k.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, P, P, P, P]
+        lib.ref_noise_site_probabilities.restype = ctypes.c_int64
+        lib.ref_noise_site_probabilities.argtypes = [P, P, ctypes.c_uint64]
         lib.ref_sample_survivors.restype = ctypes.c_int64
         lib.ref_sample_survivors.argtypes = [P, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
                                              P, P, P, P, P, P]
@@ -200,6 +204,32 @@ def ref_sample(prog, shots: int, seed: int) -> Dict[str, np.ndarray]:
     if rc != 0:
         raise RuntimeError(lib.ref_last_error().decode())
     return out
+
+
+def ref_sample_k(prog, shots: int, k: int, seed: int) -> Dict[str, np.ndarray]:
+    """The reference's clifft::sample_k (exactly k faults per shot)."""
+    lib = ref_lib()
+    out = {
+        "meas": np.zeros((shots, prog.num_measurements), np.uint8),
+        "det": np.zeros((shots, prog.num_detectors), np.uint8),
+        "obs": np.zeros((shots, prog.num_observables), np.uint8),
+        "exp_vals": np.zeros((shots, prog.num_exp_vals), np.float64),
+    }
+    rc = lib.ref_sample_k(ctypes.byref(prog.image()), shots, k, seed,
+                          *[_ptr(out[x]) for x in ("meas", "det", "obs", "exp_vals")])
+    if rc != 0:
+        raise ValueError(lib.ref_last_error().decode())
+    return out
+
+
+def ref_noise_site_probabilities(prog) -> np.ndarray:
+    lib = ref_lib()
+    cap = 1 << 20
+    buf = np.zeros(cap, np.float64)
+    n = lib.ref_noise_site_probabilities(ctypes.byref(prog.image()), buf.ctypes.data, cap)
+    if n < 0:
+        raise RuntimeError(lib.ref_last_error().decode())
+    return buf[:n].copy()
 
 
 def ref_sample_survivors(prog, shots: int, seed: int, keep_records: bool = False):

@@ -431,6 +431,36 @@ int ref_sample(const clifft_program_image* img, uint32_t shots, uint64_t seed, u
     });
 }
 
+// clifft::sample_k (src/clifft/svm/svm.cc:548-613): every shot conditioned on
+// exactly k faults. Throws (status -1, message) for strata without mass.
+int ref_sample_k(const clifft_program_image* img, uint32_t shots, uint32_t k, uint64_t seed, uint8_t* meas,
+                 uint8_t* det, uint8_t* obs, double* exp_vals) {
+    return guarded([&] {
+        auto m = module_from_image(img);
+        auto r = sample_k(*m, shots, k, seed);
+        if (meas && !r.measurements.empty()) std::memcpy(meas, r.measurements.data(), r.measurements.size());
+        if (det && !r.detectors.empty()) std::memcpy(det, r.detectors.data(), r.detectors.size());
+        if (obs && !r.observables.empty()) std::memcpy(obs, r.observables.data(), r.observables.size());
+        if (exp_vals && !r.exp_vals.empty())
+            std::memcpy(exp_vals, r.exp_vals.data(), r.exp_vals.size() * sizeof(double));
+        return 0;
+    });
+}
+
+// clifft::noise_site_probabilities (src/clifft/svm/svm.cc:356-369) into out
+// (noise sites then readout entries); returns the count.
+int64_t ref_noise_site_probabilities(const clifft_program_image* img, double* out, uint64_t cap) {
+    int64_t n = -1;
+    int rc = guarded([&] {
+        auto m = module_from_image(img);
+        auto p = noise_site_probabilities(*m);
+        for (size_t i = 0; i < p.size() && i < cap; ++i) out[i] = p[i];
+        n = int64_t(p.size());
+        return 0;
+    });
+    return rc == 0 ? n : -1;
+}
+
 // clifft::sample_survivors (src/clifft/svm/svm.cc:266-345). counts[0..2] =
 // total_shots, passed_shots, logical_errors. Record buffers must hold `shots`
 // rows; the return value is the number of rows written.
