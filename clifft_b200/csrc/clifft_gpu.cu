@@ -334,7 +334,7 @@ struct LaunchPlan {
     uint32_t nw_words;
     bool tiles;       // statevector passes stream through the bulk-copy tile engine
     bool fuse;        // ... and consecutive opcodes fuse into one pass
-    uint32_t stages;  // tile buffers per CTA (3 lets two 256-thread CTAs share an SM)
+    uint32_t stages;  // tile buffers per CTA (2 / 3 let three 128-thread / two 256-thread CTAs share an SM)
 };
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
@@ -398,11 +398,12 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
             L.threads = L.regions * 32;
         }
     } else {
-        // default: 256 threads, so two CTAs (three tile buffers each) share an SM
-        int t = group_req > 32 ? int(group_req) : 256;
+        // default: 128 threads (three CTAs with two tile buffers each share an
+        // SM) up to 8 MiB statevectors, else 256 (two CTAs, three buffers)
+        int t = group_req > 32 ? int(group_req) : (state_bytes <= (size_t(8) << 20) ? 128 : 256);
         L.threads = std::min(t, max_threads);
         L.regions = 1;
-        L.stages = L.threads <= 256 ? 3 : 4;
+        L.stages = L.threads <= 128 ? 2 : (L.threads <= 256 ? 3 : 4);
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
     L.tiles = G == 0 && !L.state_in_smem;
@@ -442,9 +443,9 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
 
 // Launch shapes the autotuner tries (group_threads encoding): sub-warp groups
 // around the heuristic width for shared-memory statevectors, warp or CTA
-// groups for L2/HBM-resident ones up to 4 MiB, and for larger statevectors a
-// 512-thread CTA with four tile buffers against two 256-thread CTAs per SM
-// with three each.
+// groups for L2/HBM-resident ones up to 4 MiB, and for larger statevectors
+// CTAs of 128 (two tile buffers, three CTAs per SM), 256 (three buffers, two
+// per SM) or 512 threads (four buffers).
 std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t precision) {
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const size_t state_bytes = (size_t(1) << p.meta.peak_rank) * amp;
@@ -454,9 +455,9 @@ std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t prec
         for (int x : {g / 2, g, g * 2})
             if (x >= 1 && x <= 32) c.push_back(uint32_t(x));
     } else if (state_bytes <= (size_t(4) << 20)) {
-        c = {32, 16, 256, 512};
+        c = {32, 16, 64, 128, 256};
     } else {
-        c = {256, 512};
+        c = {128, 256, 512};
     }
     return c;
 }
