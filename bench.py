@@ -318,6 +318,76 @@ def k_sweep(torch, flush, head_fp32, head_fp64):
     return out
 
 
+def multi_program(torch, flush):
+    """The 64 seed programs (peak k 4..18) x 10^4 shots: one launch per
+    program vs one CUDA-graph launch of the whole batch (FP32)."""
+    from clifft_b200.batch import ProgramBatch
+    import clifft_b200 as cb
+    names = sorted(n[:-4] for n in os.listdir(PROGRAMS) if n.startswith("cfg2_"))
+    progs = [load_program(n) for n in names]
+    shots = 10_000
+    b = ProgramBatch(progs, shots, precision="fp32")
+    b.run()
+    graph_ms = min(b.run(list(range(100 + 64 * i, 164 + 64 * i))) for i in range(3))
+    b.free()
+    stream = torch.cuda.current_stream()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dps = [cb.load(p) for p in progs]
+    bufs = [output_buffers(torch, p, shots, dev) for p in progs]
+    for dp, bf in zip(dps, bufs):
+        device_run(dp, shots, 1, 0, "fp32", stream, bf)
+    sep = []
+    for _ in range(3):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i, (dp, bf) in enumerate(zip(dps, bufs)):
+            device_run(dp, shots, 100 + i, 0, "fp32", stream, bf)
+        e1.record(stream)
+        e1.synchronize()
+        sep.append(e0.elapsed_time(e1))
+    total = len(progs) * shots
+    return {"programs": len(progs), "shots_each": shots, "graph_shots_per_s": total / (graph_ms / 1e3),
+            "separate_launches_shots_per_s": total / (min(sep) / 1e3), "graph_over_separate": min(sep) / graph_ms}
+
+
+def gradients():
+    """Adjoint d<P_j>/dphi_i on the rotation workload (n = 40, 32 rotations,
+    16 probes redrawn on the active axes), 256 phase vectors."""
+    import numpy as np
+    from clifft_b200 import grad as GR
+    from clifft_b200.workloads import active_probes
+    prog = active_probes(load_program("cfg4"))
+    rng = np.random.default_rng(3)
+    phases = rng.uniform(0.0, 2 * np.pi, size=(256, GR.num_rot_params(prog)))
+    out = {"program": "cfg4 (n=40, 120 Clifford layers, 32 RZ, 16 probes on active axes), 256 phase vectors"}
+    for prec in ("fp64", "fp32"):
+        GR.expval_grad(prog, phases, precision=prec)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            GR.expval_grad(prog, phases, precision=prec)
+            ts.append(time.perf_counter() - t0)
+        out[f"{prec}_vectors_per_s"] = 256 / min(ts)
+        out[f"{prec}_ms_per_call"] = 1e3 * min(ts)
+    return out
+
+
+def k_fault_sampling():
+    """sample_k_survivors on the memory grid, k = 2 faults per shot, 10^6 shots (FP32)."""
+    import clifft_b200 as cb
+    prog = load_program("cfg1")
+    cb.run(prog, 100_000, 1, precision="fp32", survivors=True, want_records=False, k_faults=2)
+    ts = []
+    for s in range(3):
+        t0 = time.perf_counter()
+        r = cb.run(prog, 1_000_000, 2 + s, precision="fp32", survivors=True, want_records=False, k_faults=2)
+        ts.append((time.perf_counter() - t0, r["kernel_ms"]))
+    wall, kms = min(ts)
+    return {"program": "cfg1", "k": 2, "shots": 1_000_000, "shots_per_s_wall": 1e6 / wall,
+            "sampling_kernel_ms": kms}
+
+
 # --------------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
@@ -439,6 +509,9 @@ def main():
                 "fp64_plain_shots_per_s": 1e9 / min(r1p["ms"]), "survivors_per_step": r1["passed"] / 2}
             extras["max_abs_prob_diff_fp32_vs_fp64"] = {
                 "k24": prob_error(HEADLINE, 8), "k16": prob_error(extras["k_sweep"]["k16"]["program"], 64)}
+            extras["multi_program_batch"] = multi_program(torch, flush)
+            extras["expval_gradients"] = gradients()
+            extras["sample_k"] = k_fault_sampling()
         if world == 1:
             cpu = cpu_baseline(HEADLINE)
     line = {

@@ -9,10 +9,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <tuple>
+#include <type_traits>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -256,6 +258,10 @@ struct clifft_gpu_program {
     uint32_t num_rot_params = 0;      // ARRAY_ROT + EXPAND_ROT instructions
     std::vector<double> fault_probs;  // per noise site its total probability, then per readout entry its flip
                                       // probability (clifft::noise_site_probabilities order)
+    // launch shapes already planned for this program (see plan_launch)
+    mutable std::mutex plan_mu;
+    mutable std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t, uint32_t, uint32_t>, std::vector<uint8_t>>
+        plan_cache;
     // Statevector slab kept between calls (mapping tens of GB afresh on every
     // call costs more than a large-k launch's own setup). One call at a time
     // holds it; a concurrent call on the same handle allocates its own.
@@ -349,9 +355,16 @@ int default_group(uint32_t peak) {
     return g;
 }
 
-LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
-                       uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words,
-                       bool allow_fusion) {
+// Everything of a plan except the grid size, which depends on the shot count
+// and (for global statevectors) on the free device memory at call time.
+struct PlanShape {
+    LaunchPlan L;
+    int per_sm;
+    int sms;
+};
+
+PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req, uint32_t rec_words,
+                     uint32_t det_words, uint32_t obs_words, bool allow_fusion) {
     LaunchPlan L{};
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const uint64_t stride = uint64_t(1) << p.meta.peak_rank;
@@ -424,6 +437,73 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     int per_sm = 0;
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)L.fn, L.threads, L.smem));
     if (per_sm < 1) invalid("kernel does not fit on an SM with this launch shape");
+    L.state_stride = stride;
+    return PlanShape{L, per_sm, sms};
+}
+
+static_assert(std::is_trivially_copyable<PlanShape>::value, "plan shapes are cached as bytes");
+
+// Per host thread and device: the event pair that times a call's kernel.
+struct CallEvents {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+};
+CallEvents& call_events(int dev) {
+    thread_local std::map<int, CallEvents> ev;
+    CallEvents& c = ev[dev];
+    if (!c.e0) {
+        CUDA_OK(cudaEventCreate(&c.e0));
+        CUDA_OK(cudaEventCreate(&c.e1));
+    }
+    return c;
+}
+
+// Calls allocate their scratch and staged records stream-ordered; the
+// device's default pool keeps up to 1 GiB of freed memory instead of
+// returning it at every synchronisation, so small repeated calls do not
+// remap memory each time. Set once per device (never lowered).
+void keep_pool_memory(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    done.push_back(dev);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    uint64_t thr = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) == cudaSuccess && thr < (1ull << 30)) {
+        thr = 1ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+}
+
+// The launch plan of one call. Shapes are planned once per (precision,
+// group request, fusion, record widths) and program, so repeated calls skip
+// the device queries; the grid is sized per call.
+LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
+                       uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words,
+                       bool allow_fusion) {
+    const auto key = std::make_tuple(precision, group_req, allow_fusion, rec_words, det_words, obs_words);
+    PlanShape ps;
+    {
+        std::lock_guard<std::mutex> lock(p.plan_mu);
+        auto it = p.plan_cache.find(key);
+        if (it != p.plan_cache.end()) {
+            std::memcpy(&ps, it->second.data(), sizeof(PlanShape));
+        } else {
+            ps = plan_shape(p, precision, group_req, rec_words, det_words, obs_words, allow_fusion);
+            std::vector<uint8_t> blob(sizeof(PlanShape));
+            std::memcpy(blob.data(), &ps, sizeof(PlanShape));
+            p.plan_cache.emplace(key, std::move(blob));
+        }
+    }
+    LaunchPlan L = ps.L;
+    const int per_sm = ps.per_sm, sms = ps.sms;
+    const uint64_t stride = L.state_stride;
+    const size_t state_bytes = stride * (precision == CLIFFT_GPU_FP32 ? 8 : 16);
     const uint64_t shots_per_block = uint64_t(L.regions) * L.S;
     const uint64_t blocks_needed = (shots + shots_per_block - 1) / shots_per_block;
     uint64_t blocks = uint64_t(per_sm) * sms;
@@ -437,7 +517,6 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
     }
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, blocks_needed));
     L.blocks = int(blocks);
-    L.state_stride = stride;
     return L;
 }
 
@@ -472,6 +551,56 @@ std::map<std::tuple<uint64_t, int, uint32_t>, uint32_t> g_tuned;
 uint64_t fnv1a(const uint8_t* p, size_t n, uint64_t h = 1469598103934665603ull) {
     for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
     return h;
+}
+
+// Persisted tuning results: with CLIFFT_GPU_TUNE_CACHE naming a file, every
+// tuned shape is appended as "program-hash device-signature mode group" and
+// earlier lines are consulted before timing trials. The device signature is
+// the device name and SM count, so a cache file may travel between machines
+// with the same GPU model.
+std::map<std::tuple<uint64_t, uint64_t, uint32_t>, uint32_t> g_tune_file;
+std::string g_tune_file_path;
+
+uint64_t device_signature(int dev) {
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return fnv1a(reinterpret_cast<const uint8_t*>(prop.name), std::strlen(prop.name)) ^
+           (uint64_t(prop.multiProcessorCount) << 48);
+}
+
+// caller holds g_tune_mu
+bool tune_file_lookup(uint64_t hash, int dev, uint32_t key, uint32_t& group) {
+    const char* path = std::getenv("CLIFFT_GPU_TUNE_CACHE");
+    if (!path || !*path) return false;
+    if (g_tune_file_path != path) {
+        g_tune_file.clear();
+        g_tune_file_path = path;
+        if (FILE* f = std::fopen(path, "r")) {
+            unsigned long long h = 0, sig = 0;
+            unsigned m = 0, g = 0;
+            while (std::fscanf(f, "%llx %llx %u %u", &h, &sig, &m, &g) == 4) g_tune_file[{h, sig, m}] = g;
+            std::fclose(f);
+        }
+    }
+    auto it = g_tune_file.find({hash, device_signature(dev), key});
+    if (it == g_tune_file.end()) return false;
+    group = it->second;
+    return true;
+}
+
+// caller holds g_tune_mu
+void tune_file_store(uint64_t hash, int dev, uint32_t key, uint32_t group) {
+    const char* path = std::getenv("CLIFFT_GPU_TUNE_CACHE");
+    if (!path || !*path) return;
+    const uint64_t sig = device_signature(dev);
+    if (FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "%016llx %016llx %u %u\n", (unsigned long long)hash, (unsigned long long)sig, key, group);
+        std::fclose(f);
+    }
+    if (g_tune_file_path == path) g_tune_file[{hash, sig, key}] = group;
 }
 
 }  // namespace
@@ -676,6 +805,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         out->kernel_ms = 0.f;
         if (shots == 0) return;
         CUDA_OK(cudaSetDevice(prog->device));
+        keep_pool_memory(prog->device);
         cudaStream_t st = static_cast<cudaStream_t>(args->stream);
         StreamBuffers buf(st);
         SlabLease slab(*prog, buf, st);
@@ -709,10 +839,15 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         if (group_req == 0 && !(args->flags & CLIFFT_GPU_NO_AUTOTUNE)) {
             std::lock_guard<std::mutex> lock(g_tune_mu);
             auto it = g_tuned.find(tune_id);
-            if (it != g_tuned.end())
+            uint32_t from_file = 0;
+            if (it != g_tuned.end()) {
                 group_req = it->second;
-            else if (shots >= kTuneMinShots)
+            } else if (tune_file_lookup(prog->content_hash, prog->device, tune_key, from_file)) {
+                g_tuned[tune_id] = from_file;
+                group_req = from_file;
+            } else if (shots >= kTuneMinShots) {
                 tune = tune_candidates(*prog, args->precision);
+            }
         }
         LaunchPlan L = plan_launch(*prog, args->precision, group_req, shots, rec_words, det_words, obs_words,
                                    allow_fusion);
@@ -822,9 +957,8 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
                 stage_out(out->final_v, K.dump_shots * (uint64_t(1) << m.peak_rank) * 16));
         }
 
-        cudaEvent_t e0, e1;
-        CUDA_OK(cudaEventCreate(&e0));
-        CUDA_OK(cudaEventCreate(&e1));
+        CallEvents& ce = call_events(prog->device);
+        cudaEvent_t e0 = ce.e0, e1 = ce.e1;
         uint32_t launches = 0;
         if (!tune.empty()) {
             // Trial launches on the first shots of this call (their records are
@@ -864,6 +998,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             {
                 std::lock_guard<std::mutex> lock(g_tune_mu);
                 g_tuned[tune_id] = best;
+                tune_file_store(prog->content_hash, prog->device, tune_key, best);
             }
             L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion);
         }
@@ -889,8 +1024,6 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         CUDA_OK(cudaStreamSynchronize(st));
         float ms = 0.f;
         CUDA_OK(cudaEventElapsedTime(&ms, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
         const uint32_t nwo = std::max<uint32_t>(m.num_words, 1);
         for (uint64_t s = 0; s < shots && !hpx.empty(); ++s)
             for (uint32_t w = 0; w < nwo; ++w) out->final_px[s * nwo + w] = hpx[s * nwt + w];

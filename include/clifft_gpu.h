@@ -32,7 +32,10 @@
  * call returns after its stream has finished the call's work. Statevectors
  * that do not fit in shared memory live in a device slab kept on the program
  * handle between calls (one call at a time uses it; a concurrent call
- * allocates its own for the call's duration).
+ * allocates its own for the call's duration). Per-call scratch and staged
+ * records come from the device's default stream-ordered memory pool, whose
+ * release threshold the library raises to 1 GiB on first use of a device so
+ * freed memory is reused instead of remapped by every call.
  */
 #ifndef CLIFFT_GPU_H
 #define CLIFFT_GPU_H
@@ -137,7 +140,10 @@ void clifft_gpu_free(clifft_gpu_program* prog);
  * shots times a few candidate launch shapes (lanes per shot, or CTA size)
  * on up to two resident waves of this call's own shots, keeps the fastest
  * for every handle of the same program content on this device (for the rest
- * of the process), and uses it from then on. Results do not depend on
+ * of the process), and uses it from then on. With the environment variable
+ * CLIFFT_GPU_TUNE_CACHE naming a file, results are also appended there and
+ * read back by later processes (keyed by program content, GPU model and
+ * mode), so trials run once per program and GPU model. Results do not depend on
  * the launch shape: every shot draws from its own Philox stream and every
  * reduction has a fixed order. Trial launches are counted in
  * kernel_launches but not in kernel_ms. */

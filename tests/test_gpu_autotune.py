@@ -49,3 +49,18 @@ def test_small_calls_do_not_tune():
     prog = _prog("cfg2_20")
     r = cb.run(prog, 200, 1, precision="fp32")
     assert r["kernel_launches"] == 1
+
+
+def test_tune_cache_file_is_written_and_read_by_a_later_process(tmp_path):
+    import subprocess
+    import sys
+    cache = tmp_path / "tune.txt"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r); import clifft_b200 as cb; from clifft_b200.program import Program; "
+            "p = Program.load(%r); r = cb.run(p, 4096, 1, precision='fp32'); print(r['kernel_launches'])"
+            % (root, os.path.join(PROGRAMS, "cfg2_15.npz")))
+    env = dict(os.environ, CLIFFT_GPU_TUNE_CACHE=str(cache))
+    first = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+    assert int(first.stdout.split()[-1]) > 1 and cache.read_text().strip()
+    second = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+    assert int(second.stdout.split()[-1]) == 1  # shape read from the file, no trials
