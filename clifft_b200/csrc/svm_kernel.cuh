@@ -1701,14 +1701,96 @@ struct Shot {
         const int tid = Grp::rank(), nthr = Grp::size();
         const int nm = n_mops;
         cur_site = 6;
+        constexpr uint32_t TN = 1u << MB;
+        const uint32_t rpt = TN / (uint32_t)nthr;  // amplitudes per thread in a register-staged run
         stream_tiles(1ull << (k - MB), C, r, 0, 0, 1u << (MB - r), [&](T* buf, uint64_t) {
-            for (int j = 0; j < nm; ++j) {
+            for (int j = 0; j < nm;) {
+                int e = j;
+                while (e < nm && index_map_kind(mops[e].kind)) ++e;
+                if (e - j >= 2 && rpt <= kMaxRunAmps) {
+                    if (rpt == 16)
+                        apply_index_run<16>(mops, j, e, buf, tid, nthr);
+                    else if (rpt == 8)
+                        apply_index_run<8>(mops, j, e, buf, tid, nthr);
+                    else
+                        apply_index_run<4>(mops, j, e, buf, tid, nthr);
+                    j = e;
+                    continue;
+                }
                 apply_micro(mops[j], buf, tid, nthr);
                 __syncthreads();
+                ++j;
             }
         });
         moved += (2ull << k) * sizeof(T);
         return end - pc;
+    }
+
+    // Micro-ops that map every amplitude to one position (CNOT, SWAP,
+    // multi-CNOT: bit maps on the tile index) and / or multiply it by a
+    // factor that depends on its position (CZ, multi-CZ, PHASE).
+    static __device__ __forceinline__ bool index_map_kind(uint8_t kind) {
+        return kind == M_CNOT || kind == M_SWAP || kind == M_MCNOT || kind == M_CZ || kind == M_MCZ ||
+               kind == M_PHASE;
+    }
+    static constexpr uint32_t kMaxRunAmps = sizeof(R) == 4 ? 16u : 8u;  // register budget of a staged run
+    // A run mops[j0, j1) of index-map micro-ops in one pass over the tile: each
+    // thread reads RPT amplitudes into registers, follows every amplitude's
+    // position through the run, applying the diagonal factors in the run's
+    // order (the same operations, in the same order, as one micro-op at a
+    // time), then writes each amplitude at its final position. The barrier
+    // between the read and write phases makes the in-place permutation safe.
+    template <int RPT>
+    static __device__ void apply_index_run(const MicroOp* mops, int j0, int j1, T* tile, int tid, int nthr) {
+        T v[RPT];
+        uint32_t pos[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+            pos[q] = (uint32_t)(tid + q * nthr);
+            v[q] = tile[pos[q]];
+        }
+        for (int j = j0; j < j1; ++j) {
+            const MicroOp& m = mops[j];
+            const uint32_t ab = 1u << m.a, bb = 1u << m.b;
+            switch (m.kind) {
+                case M_CNOT:
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if (pos[q] & ab) pos[q] ^= bb;
+                    break;
+                case M_SWAP:
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if (((pos[q] >> m.a) ^ (pos[q] >> m.b)) & 1u) pos[q] ^= ab | bb;
+                    break;
+                case M_MCNOT:
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if (__popc(pos[q] & m.mask & ~ab) & 1) pos[q] ^= ab;
+                    break;
+                case M_CZ:
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if ((pos[q] & ab) && (pos[q] & bb)) v[q] = cneg(v[q]);
+                    break;
+                case M_MCZ:
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if ((pos[q] & ab) && (__popc(pos[q] & m.mask) & 1)) v[q] = cneg(v[q]);
+                    break;
+                default: {  // M_PHASE
+                    const T ph = Cx<R>::make(m.c[0], m.c[1]);
+#pragma unroll
+                    for (int q = 0; q < RPT; ++q)
+                        if (pos[q] & ab) v[q] = cmul(v[q], ph);
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) tile[pos[q]] = v[q];
+        __syncthreads();
     }
 
     // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes; the
