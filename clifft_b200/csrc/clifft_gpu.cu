@@ -405,7 +405,11 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
     if (G) {
         L.threads = std::min(128, max_threads);
         L.regions = L.threads / 32;
-        L.state_in_smem = region_bytes(true) + tail(32) <= smem_cap;
+        // shared-memory statevectors only while at least 8 warps fit on an SM;
+        // larger ones run from global memory (L2 / HBM) with full occupancy
+        int smem_sm = 0;
+        CUDA_OK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        L.state_in_smem = region_bytes(true) + tail(32) <= smem_cap && region_bytes(true) * 8 <= size_t(smem_sm);
         while (L.regions > 1 && region_bytes(L.state_in_smem) * L.regions + tail(L.threads) > smem_cap) {
             L.regions /= 2;
             L.threads = L.regions * 32;
