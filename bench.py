@@ -305,13 +305,15 @@ def k_sweep(torch, flush, head_fp32, head_fp64):
         prog = load_program(name)
         row = {"program": name, "shots": shots}
         for prec, plain in (("fp32", False), ("fp64", True)):
-            r = time_device(torch, prog, shots, prec, steps=2, warmup=2, rank=0, flush=flush, plain=plain)
+            r = time_device(torch, prog, shots, prec, steps=3, warmup=2, rank=0, flush=flush, plain=plain)
             kms = min(r["kernel_ms"])
             key = "fp32_batched" if prec == "fp32" else "fp64_plain"
-            row[f"{key}_shots_per_s"] = shots / (min(r["ms"]) / 1e3)
+            row[f"{key}_shots_per_s"] = shots / (statistics.median(r["ms"]) / 1e3)
+            row[f"{key}_kernel_shots_per_s"] = shots / (kms / 1e3)
             row[f"{key}_alg_GBps"] = (r["alg_bytes"] / len(r["ms"])) / (kms / 1e3) / 1e9
             row[f"{key}_group_threads"] = r["group_threads"]
         row["fp32_over_fp64"] = row["fp32_batched_shots_per_s"] / row["fp64_plain_shots_per_s"]
+        row["fp32_over_fp64_kernel"] = row["fp32_batched_kernel_shots_per_s"] / row["fp64_plain_kernel_shots_per_s"]
         out[f"k{k}"] = row
     out["k24"] = {"program": HEADLINE, "shots": SHOTS_PER_GPU, "fp32_batched_shots_per_s": head_fp32,
                   "fp64_plain_shots_per_s": head_fp64, "fp32_over_fp64": head_fp32 / head_fp64}
