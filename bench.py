@@ -179,7 +179,7 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survi
             "alg_bytes": alg_bytes, "streamed_bytes": streamed, "group_threads": sorted(groups)}
 
 
-def time_e2e(name, shots, steps, torch):
+def time_e2e(name, shots, steps, torch, first_shot=0):
     """Public-API path with host buffers: fresh upload of the program image
     (H2D), sampling, packed records read back (D2H) and unpacked to numpy."""
     import clifft_b200 as cb
@@ -190,7 +190,7 @@ def time_e2e(name, shots, steps, torch):
         prog = Program.load(path)  # host-side program, not yet on the device
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        cb.sample(prog, shots, seed=50 + s, precision="fp32")
+        cb.sample(prog, shots, seed=50 + s, precision="fp32", first_shot=first_shot)
         dt = time.perf_counter() - t0
         if s == 0:
             continue  # first call pays one-time CUDA context / kernel attribute setup
@@ -487,14 +487,23 @@ def main():
             traffic = None
 
     extras = {}
-    e2e = None
     cpu = None
+    # end to end on every rank (each samples its own shots through the public
+    # API); the step time is the slowest rank's
+    barrier()
+    e_times, h2d, d2h = time_e2e(HEADLINE, SHOTS_PER_GPU, max(2, min(args.steps, 3)), torch,
+                                 first_shot=rank * SHOTS_PER_GPU)
+    e_ms = 1e3 * sum(e_times) / len(e_times)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e = {"value": SHOTS_PER_GPU * world / (e_ms / 1e3), "unit": "shots/s",
+           "h2d_bytes_per_step": int(h2d) * world, "d2h_bytes_per_step": int(d2h) * world,
+           "ms_per_step": e_ms}
     if rank == 0:
-        e_times, h2d, d2h = time_e2e(HEADLINE, SHOTS_PER_GPU, max(2, min(args.steps, 3)), torch)
-        e2e = {"value": SHOTS_PER_GPU / (sum(e_times) / len(e_times)), "unit": "shots/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": 1e3 * sum(e_times) / len(e_times)}
-        if not args.no_extras:
+        if not args.no_extras and world == 1:  # single-GPU comparisons; an N-GPU run holds all N GPUs
             r64 = time_device(torch, prog, SHOTS_PER_GPU, "fp64", 2, 1, 0, flush, plain=True)
             fp64 = SHOTS_PER_GPU / (min(r64["ms"]) / 1e3)
             extras["fp64_plain_executor_shots_per_s"] = fp64

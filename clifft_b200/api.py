@@ -190,14 +190,15 @@ def _stats(r) -> dict:
 
 
 def sample(program: Program, shots: int, seed: Optional[int] = None, *,
-           precision: str = "fp32", group_threads: int = 0) -> SampleResult:
-    """clifft.sample (src/clifft/svm/svm.cc:191-255) on the GPU."""
+           precision: str = "fp32", group_threads: int = 0, first_shot: int = 0) -> SampleResult:
+    """clifft.sample (src/clifft/svm/svm.cc:191-255) on the GPU. `first_shot`
+    offsets the per-shot streams (a shard of a larger run)."""
     if program.has_postselection:
         raise ValueError(
             "sample() cannot be used with post-selected programs because it returns a fixed "
             "number of rows and cannot discard shots. Use sample_survivors(program, shots, "
             "keep_records=True) instead.")
-    r = run(program, shots, seed, precision=precision, group_threads=group_threads)
+    r = run(program, shots, seed, precision=precision, group_threads=group_threads, first_shot=first_shot)
     return SampleResult(_unpack(r["meas_words"], program.num_measurements),
                         _unpack(r["det_words"], program.num_detectors),
                         _unpack(r["obs_words"], program.num_observables),
