@@ -25,6 +25,7 @@ CLIFFT_GPU_NO_FUSION = 0x20
 CLIFFT_GPU_FORCE_FUSION = 0x40
 CLIFFT_GPU_PROFILE = 0x80
 CLIFFT_GPU_NO_AUTOTUNE = 0x100
+CLIFFT_GPU_NO_SEGMENTS = 0x200
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device error", -4: "out of memory"}
 

@@ -87,7 +87,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         readout_faults: Optional[Sequence[Sequence[int]]] = None, trace: bool = False,
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
-        profile: bool = False, autotune: bool = True, k_faults: Optional[int] = None) -> Dict[str, object]:
+        profile: bool = False, autotune: bool = True, k_faults: Optional[int] = None,
+        segments: bool = True) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None / True = runs of
     consecutive opcodes share one pass over a global-memory statevector,
@@ -132,6 +133,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_PROFILE
     if not autotune:
         flags |= N.CLIFFT_GPU_NO_AUTOTUNE
+    if not segments:
+        flags |= N.CLIFFT_GPU_NO_SEGMENTS
     if fusion is False:
         flags |= N.CLIFFT_GPU_NO_FUSION
     elif fusion is True:

@@ -546,6 +546,26 @@ std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t prec
 }
 
 constexpr uint64_t kTuneMinShots = 1024;
+constexpr uint32_t kSegHeaderBytes = 192;  // saved-state header of a shot between segments (svm_kernel.cuh)
+constexpr uint32_t kMaxSegments = 8;
+
+// Instruction cuts [0, c1, ..., n] for segmented survivor runs: each inner
+// cut follows a POSTSELECT, at about equal numbers of POSTSELECTs per
+// segment. Fewer than two POSTSELECTs give no inner cut.
+std::vector<uint32_t> segment_cuts(const clifft_gpu_program& p) {
+    std::vector<uint32_t> post;
+    const uint32_t n = p.meta.num_instructions;
+    for (uint32_t i = 0; i < n; ++i)
+        if (p.instr_host[size_t(i) * 32] == CLIFFT_OP_POSTSELECT) post.push_back(i);
+    std::vector<uint32_t> cuts{0};
+    const uint32_t m = std::min<uint32_t>(kMaxSegments, uint32_t(post.size()));
+    for (uint32_t j = 1; j < m; ++j) {
+        const uint32_t c = post[size_t(j) * post.size() / m - 1] + 1;
+        if (c > cuts.back() && c < n) cuts.push_back(c);
+    }
+    cuts.push_back(n);
+    return cuts;
+}
 
 // Launch shapes picked by the autotuner, shared by every handle of the same
 // program content in this process: (content hash, device, precision/mode).
@@ -1007,9 +1027,47 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion);
         }
         apply_plan(K, L);
+        // Survivor runs of warp groups go segment by segment: the program is cut
+        // after POSTSELECT opcodes, and only the shots still alive at a cut are
+        // carried (state saved, ids compacted) into the next segment, so warps
+        // are not left running lanes whose shot was already discarded.
+        const std::vector<uint32_t> cuts =
+            (args->flags & CLIFFT_GPU_SURVIVORS) && !(args->flags & CLIFFT_GPU_NO_SEGMENTS) && L.G > 0 &&
+                    !(args->flags & CLIFFT_GPU_TRACE) && !profile &&
+                    shots >= 4 * uint64_t(L.blocks) * L.regions * L.S
+                ? segment_cuts(*prog)
+                : std::vector<uint32_t>();
         CUDA_OK(cudaEventRecord(e0, st));
-        L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
-        CUDA_OK(cudaGetLastError());
+        if (cuts.size() < 3) {
+            L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
+            CUDA_OK(cudaGetLastError());
+        } else {
+            const uint32_t nseg = uint32_t(cuts.size() - 1);
+            const uint32_t nwords = rec_words + det_words + obs_words;
+            const uint64_t stride = (kSegHeaderBytes + ((nwords * 4u + 15u) & ~15u) +
+                                     (uint64_t(1) << m.peak_rank) * amp + 15u) & ~uint64_t(15);
+            K.seg_state = static_cast<unsigned char*>(buf.alloc(size_t(shots) * stride));
+            K.seg_stride = stride;
+            uint32_t* lists[2] = {static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4)),
+                                  static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4))};
+            auto* segc = static_cast<unsigned long long*>(buf.alloc(size_t(nseg) * 2 * 8));
+            CUDA_OK(cudaMemsetAsync(segc, 0, size_t(nseg) * 2 * 8, st));
+            for (uint32_t sgi = 0; sgi < nseg; ++sgi) {
+                KParams Ks = K;
+                Ks.seg_flags = KSEG_ON | (sgi == 0 ? KSEG_FIRST : 0u) | (sgi + 1 == nseg ? KSEG_LAST : 0u);
+                Ks.seg_begin = cuts[sgi];
+                Ks.seg_end = cuts[sgi + 1];
+                Ks.seg_in = sgi == 0 ? nullptr : lists[(sgi + 1) & 1];
+                Ks.seg_count_in = sgi == 0 ? nullptr : segc + (sgi - 1);
+                Ks.seg_out = lists[sgi & 1];
+                Ks.seg_count_out = segc + sgi;
+                if (sgi > 0) Ks.work_counter = segc + nseg + sgi;  // a fresh work counter per launch
+                L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, Ks);
+                CUDA_OK(cudaGetLastError());
+                ++launches;
+            }
+            --launches;  // the first segment is the call's regular launch
+        }
         CUDA_OK(cudaEventRecord(e1, st));
 
         for (auto& o : outs) CUDA_OK(cudaMemcpyAsync(o.host, o.dev, o.bytes, cudaMemcpyDeviceToHost, st));

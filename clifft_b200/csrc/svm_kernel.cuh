@@ -126,6 +126,17 @@ struct KParams {
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
     uint32_t stages;      // tile buffers per CTA (2..kMaxStages) when fuse_bytes != 0
     unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
+    // segmented execution (survivor runs of warp groups): this launch runs
+    // instructions [seg_begin, seg_end) for the items of seg_in; shots alive
+    // at seg_end save their state and append themselves to seg_out
+    uint32_t seg_flags;                       // KSEG_* (0 = the whole program in one launch)
+    uint32_t seg_begin, seg_end;
+    const uint32_t* seg_in;                   // shot ids of this segment's items (null: item = shot)
+    const unsigned long long* seg_count_in;   // number of items (null: shots)
+    uint32_t* seg_out;
+    unsigned long long* seg_count_out;
+    unsigned char* seg_state;                 // per shot: saved state, seg_stride bytes
+    uint64_t seg_stride;
 };
 
 enum : uint32_t {
@@ -134,6 +145,12 @@ enum : uint32_t {
     KF_FORCED_FAULTS = 0x04u,
     KF_TRACE = 0x10u,
     KF_FUSE = 0x20u,  // fused tile sweeps for global-memory statevectors (CTA groups)
+};
+
+enum : uint32_t {
+    KSEG_ON = 0x1u,     // segmented launch
+    KSEG_FIRST = 0x2u,  // shots start from the reset state
+    KSEG_LAST = 0x4u,   // shots alive at the end are finished (records written)
 };
 
 enum : int {
@@ -2038,6 +2055,119 @@ struct Shot {
 
     // ------------------------------------------------------------ driver
     __device__ __forceinline__ void run(Tally& tally) {
+        const bool seg = (K.seg_flags & KSEG_ON) != 0;
+        if (seg && !(K.seg_flags & KSEG_FIRST)) {
+            load_state();
+        } else {
+            reset();
+        }
+        const uint32_t n_instr = P.n_instr;
+        const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) != 0;
+        const bool prof = K.phase_cycles != nullptr && Grp::rank() == 0;
+        if (Grp::kCta) {
+            run_cta(fuse_on, prof);
+        } else {
+            const uint32_t end = seg ? K.seg_end : n_instr;
+            for (uint32_t pc = seg ? K.seg_begin : 0; pc < end; ++pc) {
+                pc = frame_run(pc, end);
+                if (pc >= end) break;
+                exec(pc);
+                if (stop) break;
+            }
+        }
+        Grp::sync();
+        if (seg && !(K.seg_flags & KSEG_LAST) && !stop) {
+            save_state();
+            return;
+        }
+        finish(tally);
+    }
+
+    // Saved state of a shot between segments: frame, gamma, counters and
+    // cursors, the packed records, and the 2^k active amplitudes.
+    static __host__ __device__ constexpr uint32_t seg_header_bytes() { return 192u; }
+    __device__ __forceinline__ void save_state() {
+        flush_records();
+        unsigned char* d = K.seg_state + shot * K.seg_stride;
+        const int r = Grp::rank();
+        if (r == 0) {
+            uint64_t* w = reinterpret_cast<uint64_t*>(d);
+#pragma unroll
+            for (int i = 0; i < NW; ++i) {
+                w[i] = f.x[i];
+                w[NW + i] = f.z[i];
+            }
+            double* dd = reinterpret_cast<double*>(d + 64);
+            dd[0] = gamma.x;
+            dd[1] = gamma.y;
+            dd[2] = log_prob;
+            unsigned long long* u = reinterpret_cast<unsigned long long*>(d + 88);
+            u[0] = dust;
+            u[1] = bytes;
+            u[2] = moved;
+            uint32_t* q = reinterpret_cast<uint32_t*>(d + 112);
+            q[0] = k;
+            q[1] = draw;
+            q[2] = next_noise;
+            q[3] = ff_pos;
+            q[4] = ff_end;
+            q[5] = ro_pos;
+            q[6] = ro_end;
+            q[7] = (discarded ? 2u : 0u) | (reachable ? 4u : 0u);
+        }
+        uint32_t* words = reinterpret_cast<uint32_t*>(d + seg_header_bytes());
+        const uint32_t nwords = K.rec_words + K.det_words + K.obs_words;
+        for (uint32_t i = r; i < nwords; i += Grp::size()) words[i] = rec[i * S];
+        T* amps = reinterpret_cast<T*>(d + seg_header_bytes() + ((nwords * 4u + 15u) & ~15u));
+        for (uint64_t i = r; i < (1ull << k); i += Grp::size()) amps[i] = A(i);
+        Grp::sync();
+        if (r == 0) {
+            const unsigned long long at = atomicAdd(K.seg_count_out, 1ull);
+            K.seg_out[at] = (uint32_t)shot;
+        }
+    }
+    __device__ __forceinline__ void load_state() {
+        const unsigned char* d = K.seg_state + shot * K.seg_stride;
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(d);
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+            f.x[i] = w[i];
+            f.z[i] = w[NW + i];
+        }
+        const double* dd = reinterpret_cast<const double*>(d + 64);
+        gamma = make_double2(dd[0], dd[1]);
+        log_prob = dd[2];
+        const unsigned long long* u = reinterpret_cast<const unsigned long long*>(d + 88);
+        dust = u[0];
+        bytes = u[1];
+        moved = u[2];
+        const uint32_t* q = reinterpret_cast<const uint32_t*>(d + 112);
+        k = q[0];
+        draw = q[1];
+        next_noise = q[2];
+        ff_pos = q[3];
+        ff_end = q[4];
+        ro_pos = q[5];
+        ro_end = q[6];
+        stop = false;
+        discarded = (q[7] & 2u) != 0;
+        reachable = (q[7] & 4u) != 0;
+        resolving = false;
+        solo = false;
+        n_mops = 0;
+        rec_dirty = false;
+        forced = (K.flags & KF_FORCED_MEAS) ? K.forced_meas + shot * P.slots : nullptr;
+        meas_prob = nullptr;
+        const int r = Grp::rank();
+        const uint32_t* words = reinterpret_cast<const uint32_t*>(d + seg_header_bytes());
+        const uint32_t nwords = K.rec_words + K.det_words + K.obs_words;
+        for (uint32_t i = r; i < nwords; i += Grp::size()) rec[i * S] = words[i];
+        const T* amps = reinterpret_cast<const T*>(d + seg_header_bytes() + ((nwords * 4u + 15u) & ~15u));
+        for (uint64_t i = r; i < (1ull << k); i += Grp::size()) A(i) = amps[i];
+        Grp::sync();
+    }
+
+    __device__ __forceinline__ void reset() {
         // SchrodingerState::reset (svm_state.cc:220-267): only v[0] needs a
         // value; every other amplitude is written by EXPAND before it is read.
         f.clear();
@@ -2078,22 +2208,6 @@ struct Shot {
             draw_next_noise();
         }
         Grp::sync();
-
-        const uint32_t n_instr = P.n_instr;
-        const bool fuse_on = Grp::kCta && (K.flags & KF_FUSE) != 0;
-        const bool prof = K.phase_cycles != nullptr && Grp::rank() == 0;
-        if (Grp::kCta) {
-            run_cta(fuse_on, prof);
-        } else {
-            for (uint32_t pc = 0; pc < n_instr; ++pc) {
-                pc = frame_run(pc, n_instr);
-                if (pc >= n_instr) break;
-                exec(pc);
-                if (stop) break;
-            }
-        }
-        Grp::sync();
-        finish(tally);
     }
 
     __device__ __forceinline__ void finish(Tally& tally) {
@@ -2222,6 +2336,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
         v = reinterpret_cast<T*>(K.state_global) + gid * K.state_stride * S + Grp::slot();
     }
     Tally tally;
+    const unsigned long long n_items = K.seg_count_in ? *K.seg_count_in : K.shots;
     for (;;) {
         unsigned long long base = 0;
         if (Grp::kCta) {
@@ -2234,9 +2349,10 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
             if ((threadIdx.x & 31) == 0) base = atomicAdd(K.work_counter, (unsigned long long)S);
             base = __shfl_sync(0xffffffffu, base, 0);
         }
-        if (base >= K.shots) break;
-        const unsigned long long shot = base + Grp::slot();
-        if (shot < K.shots) {
+        if (base >= n_items) break;
+        const unsigned long long item = base + Grp::slot();
+        if (item < n_items) {
+            const unsigned long long shot = K.seg_in ? (unsigned long long)K.seg_in[item] : item;
             Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, fz, &bar_phase, shot);
             s.run(tally);
         }

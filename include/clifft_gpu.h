@@ -71,6 +71,7 @@ extern "C" {
 #define CLIFFT_GPU_FORCE_FUSION 0x40u   /* reserved (fusion is on unless CLIFFT_GPU_NO_FUSION) */
 #define CLIFFT_GPU_PROFILE 0x80u        /* fill phase_cycles (adds timing atomics; not for benchmarks) */
 #define CLIFFT_GPU_NO_AUTOTUNE 0x100u   /* group_threads == 0: use the built-in heuristic, no trial launches */
+#define CLIFFT_GPU_NO_SEGMENTS 0x200u   /* survivor runs: one launch, no compaction between POSTSELECT segments */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
 
@@ -135,6 +136,11 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
  * sampling calls keep on it between calls. */
 void clifft_gpu_free(clifft_gpu_program* prog);
 /* Sample. See the flags above for survivors / forced / trace behaviour.
+ * Survivor compaction: with CLIFFT_GPU_SURVIVORS, at least four resident waves
+ * of shots and one warp (or less) per shot, the program is cut into up to 8
+ * segments after POSTSELECT opcodes; shots still alive at a cut save their
+ * state and are compacted into the next segment's launch, so warps carry only
+ * live shots. Records and counters are those of a single launch.
  * Autotuning: with group_threads == 0 and no CLIFFT_GPU_NO_AUTOTUNE, the
  * first call of a (precision, mode) pair on a program with at least 1024
  * shots times a few candidate launch shapes (lanes per shot, or CTA size)
