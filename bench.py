@@ -118,14 +118,15 @@ class ClockSampler:
 def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False, group=0):
     """One device-resident sampling step: program resident, outputs in HBM.
     plain = the plain executor: one pass per opcode, fixed heuristic launch
-    shape (no fusion, no autotuning)."""
+    shape, one launch per call (no fusion, no autotuning, no survivor
+    compaction)."""
     import ctypes
     from clifft_b200 import _native as N
     flags = N.CLIFFT_GPU_DEVICE_PTRS
     if survivors:
         flags |= N.CLIFFT_GPU_SURVIVORS
     if plain:
-        flags |= N.CLIFFT_GPU_NO_FUSION | N.CLIFFT_GPU_NO_AUTOTUNE
+        flags |= N.CLIFFT_GPU_NO_FUSION | N.CLIFFT_GPU_NO_AUTOTUNE | N.CLIFFT_GPU_NO_SEGMENTS
     a = N.SampleArgs(shots=shots, seed=seed, first_shot=first_shot,
                      precision=N.CLIFFT_GPU_FP32 if precision == "fp32" else N.CLIFFT_GPU_FP64,
                      flags=flags, group_threads=group, stream=stream.cuda_stream)
