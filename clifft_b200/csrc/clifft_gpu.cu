@@ -1037,21 +1037,26 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
                     shots >= 4 * uint64_t(L.blocks) * L.regions * L.S
                 ? segment_cuts(*prog)
                 : std::vector<uint32_t>();
-        CUDA_OK(cudaEventRecord(e0, st));
-        if (cuts.size() < 3) {
-            L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
-            CUDA_OK(cudaGetLastError());
-        } else {
-            const uint32_t nseg = uint32_t(cuts.size() - 1);
+        // segment buffers are set up ahead of the timed region
+        const uint32_t nseg = cuts.size() < 3 ? 0u : uint32_t(cuts.size() - 1);
+        uint32_t* lists[2] = {nullptr, nullptr};
+        unsigned long long* segc = nullptr;
+        if (nseg) {
             const uint32_t nwords = rec_words + det_words + obs_words;
             const uint64_t stride = (kSegHeaderBytes + ((nwords * 4u + 15u) & ~15u) +
                                      (uint64_t(1) << m.peak_rank) * amp + 15u) & ~uint64_t(15);
             K.seg_state = static_cast<unsigned char*>(buf.alloc(size_t(shots) * stride));
             K.seg_stride = stride;
-            uint32_t* lists[2] = {static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4)),
-                                  static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4))};
-            auto* segc = static_cast<unsigned long long*>(buf.alloc(size_t(nseg) * 2 * 8));
+            lists[0] = static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4));
+            lists[1] = static_cast<uint32_t*>(buf.alloc(size_t(shots) * 4));
+            segc = static_cast<unsigned long long*>(buf.alloc(size_t(nseg) * 2 * 8));
             CUDA_OK(cudaMemsetAsync(segc, 0, size_t(nseg) * 2 * 8, st));
+        }
+        CUDA_OK(cudaEventRecord(e0, st));
+        if (!nseg) {
+            L.fn<<<L.blocks, L.threads, L.smem, st>>>(prog->dev, K);
+            CUDA_OK(cudaGetLastError());
+        } else {
             for (uint32_t sgi = 0; sgi < nseg; ++sgi) {
                 KParams Ks = K;
                 Ks.seg_flags = KSEG_ON | (sgi == 0 ? KSEG_FIRST : 0u) | (sgi + 1 == nseg ? KSEG_LAST : 0u);
