@@ -1034,7 +1034,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         const std::vector<uint32_t> cuts =
             (args->flags & CLIFFT_GPU_SURVIVORS) && !(args->flags & CLIFFT_GPU_NO_SEGMENTS) && L.G > 0 &&
                     !(args->flags & CLIFFT_GPU_TRACE) && !profile &&
-                    shots >= 4 * uint64_t(L.blocks) * L.regions * L.S
+                    shots >= 4 * uint64_t(L.blocks) * L.regions * L.S && shots <= 0xffffffffull
                 ? segment_cuts(*prog)
                 : std::vector<uint32_t>();
         // segment buffers are set up ahead of the timed region
