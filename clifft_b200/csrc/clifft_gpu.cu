@@ -345,6 +345,13 @@ struct LaunchPlan {
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
 
+// Shared-memory scratch of the tile engine for one shot group.
+uint32_t tile_scratch_bytes(uint32_t precision, bool cta, uint32_t stages) {
+    if (precision == CLIFFT_GPU_FP32)
+        return cta ? TileCfg<float, true>::smem_bytes(stages) : TileCfg<float, false>::smem_bytes(stages);
+    return cta ? TileCfg<double, true>::smem_bytes(stages) : TileCfg<double, false>::smem_bytes(stages);
+}
+
 // Shot-group width for one warp: about 32 amplitudes per lane, so each warp
 // carries 32 / G shots whose statevectors interleave in 8 KiB (FP32) /
 // 16 KiB (FP64) of shared memory.
@@ -393,10 +400,12 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
     cudaFuncAttributes fa{};
     CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
     const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
+    // one-shot groups (a CTA, or a warp of 32 lanes) stream global
+    // statevectors through the tile engine: three 4 KiB buffers per warp
+    L.stages = G == 32 ? 3 : 0;
     auto region_bytes = [&](bool in_smem) {
-        size_t fuse = 0;  // tile-engine scratch: every CTA group with a global-memory statevector
-        if (G == 0 && !in_smem)
-            fuse = precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(L.stages) : fuse_smem_bytes<double>(L.stages);
+        size_t fuse = 0;  // tile-engine scratch of the group
+        if ((G == 0 || G == 32) && !in_smem) fuse = tile_scratch_bytes(precision, G == 0, L.stages);
         return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
                ~size_t(15);
     };
@@ -423,7 +432,8 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
         L.stages = L.threads <= 128 ? 2 : (L.threads <= 256 ? 3 : 4);
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
-    L.tiles = G == 0 && !L.state_in_smem;
+    L.tiles = (G == 0 || G == 32) && !L.state_in_smem;
+    if (!L.tiles) L.stages = 0;
     L.fuse = L.tiles && allow_fusion;
     L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
@@ -893,9 +903,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         // launch-shape dependent parameters (and the statevector slab)
         auto apply_plan = [&](KParams& Kx, const LaunchPlan& Lx) {
             Kx.flags = (K.flags & ~uint32_t(KF_FUSE)) | (Lx.fuse ? KF_FUSE : 0);
-            Kx.fuse_bytes = Lx.tiles ? (args->precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(Lx.stages)
-                                                                          : fuse_smem_bytes<double>(Lx.stages))
-                                     : 0;
+            Kx.fuse_bytes = Lx.tiles ? tile_scratch_bytes(args->precision, Lx.G == 0, Lx.stages) : 0;
             Kx.stages = Lx.stages;
             Kx.state_in_smem = Lx.state_in_smem ? 1 : 0;
             Kx.state_stride = Lx.state_stride;
@@ -1390,9 +1398,7 @@ int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_s
             K.flags = (a.flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
                       (a.flags & CLIFFT_GPU_FORCED_MEAS ? KF_FORCED_MEAS : 0) |
                       (a.flags & CLIFFT_GPU_FORCED_FAULTS ? KF_FORCED_FAULTS : 0) | (it.L.fuse ? KF_FUSE : 0);
-            K.fuse_bytes = it.L.tiles ? (a.precision == CLIFFT_GPU_FP32 ? fuse_smem_bytes<float>(it.L.stages)
-                                                                       : fuse_smem_bytes<double>(it.L.stages))
-                                      : 0;
+            K.fuse_bytes = it.L.tiles ? tile_scratch_bytes(a.precision, it.L.G == 0, it.L.stages) : 0;
             K.stages = it.L.stages;
             K.rec_words = rec_words;
             K.det_words = det_words;

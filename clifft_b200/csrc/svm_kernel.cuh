@@ -403,24 +403,27 @@ struct MicroOp {
     uint32_t mask;  // local-bit mask (multi gates)
     double c[32];   // up to 16 complex coefficients
 };
-constexpr int kMaxMicroOps = 24;
-constexpr int kMaxStages = 4;      // tile buffers (tiles in flight) per CTA: 2..4, chosen per launch
+constexpr int kMaxStages = 4;      // tile buffers (tiles in flight) per shot group: 2..4, chosen per launch
 constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
-template <typename R>
+// Tile-engine geometry of a one-shot group. A CTA streams 32 KiB tiles and
+// fuses up to 24 opcodes per pass; a warp running one shot streams 4 KiB
+// tiles and fuses up to 8, so that three buffers per warp leave room for
+// three 4-warp CTAs per SM. Scratch layout of one group: [kMaxStages
+// mbarriers][micro-ops][64 run offsets][64-byte axis -> local bit table]
+// [stages tile buffers, 128-B aligned].
+template <typename R, bool CTA>
 struct TileCfg {
-    static constexpr int kBits = sizeof(R) == 4 ? 12 : 11;  // 32 KiB per tile buffer
+    static constexpr int kBits = CTA ? (sizeof(R) == 4 ? 12 : 11) : (sizeof(R) == 4 ? 9 : 8);
+    static constexpr int kMops = CTA ? 24 : 8;
+    static constexpr uint32_t kBarOffset = 0;
+    static constexpr uint32_t kMopsOffset = kMaxStages * 8u;
+    static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MicroOp);
+    static constexpr uint32_t kLbitOffset = kTablesOffset + 64u * 8u;
+    static constexpr uint32_t kBufOffset = (kLbitOffset + 64u + 127u) & ~127u;
+    static __host__ __device__ constexpr uint32_t smem_bytes(uint32_t stages) {
+        return kBufOffset + stages * (1u << kBits) * 2u * (uint32_t)sizeof(R);
+    }
 };
-// Tile-engine scratch of one CTA: [kMaxStages mbarriers][micro-ops][64 run
-// offsets][64-byte axis -> local bit table][stages tile buffers, 128-B aligned]
-constexpr uint32_t kFuseBarOffset = 0;
-constexpr uint32_t kFuseMopsOffset = kMaxStages * 8u;
-constexpr uint32_t kFuseTablesOffset = kFuseMopsOffset + kMaxMicroOps * (uint32_t)sizeof(MicroOp);
-constexpr uint32_t kFuseLbitOffset = kFuseTablesOffset + 64u * 8u;
-constexpr uint32_t kFuseBufOffset = (kFuseLbitOffset + 64u + 127u) & ~127u;
-template <typename R>
-__host__ __device__ constexpr uint32_t fuse_smem_bytes(uint32_t stages) {
-    return kFuseBufOffset + stages * (1u << TileCfg<R>::kBits) * 2u * (uint32_t)sizeof(R);
-}
 
 // ---- bulk-copy (TMA, untiled) and mbarrier primitives. Every copy here reads
 // or writes this GPU's own global memory; none uses cluster multicast.
@@ -454,7 +457,7 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src_smem, uint
                  : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
@@ -490,6 +493,10 @@ template <typename R, class Grp, int NW>
 struct Shot {
     using T = typename Cx<R>::T;
     static constexpr int S = Grp::S;
+    // one-shot groups (a CTA, or a warp of 32 lanes) stream global
+    // statevectors through the tile engine
+    static constexpr bool kTiles = Grp::S == 1;
+    using TC = TileCfg<R, Grp::kCta>;
     const DevProg& P;
     const KParams& K;
     T* v;           // slot base: amplitude i at v[i * S]
@@ -701,10 +708,10 @@ struct Shot {
     __device__ __forceinline__ uint8_t local_bit(uint32_t axis) const {
         return reinterpret_cast<const uint8_t*>(fuse + fuse_lbit_offset())[axis];
     }
-    static __host__ __device__ constexpr uint32_t fuse_bar_offset() { return kFuseBarOffset; }
-    static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return kFuseMopsOffset; }
-    static __host__ __device__ constexpr uint32_t fuse_tables_offset() { return kFuseTablesOffset; }
-    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return kFuseLbitOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_bar_offset() { return TC::kBarOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return TC::kMopsOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_tables_offset() { return TC::kTablesOffset; }
+    static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return TC::kLbitOffset; }
     __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
                                          int nc) {
         if (Grp::rank() == 0) {
@@ -723,7 +730,7 @@ struct Shot {
     // exec_array_cnot (svm_kernels.inl:124-252)
     __device__ __forceinline__ void array_cnot(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), cb = 1ull << c, tb = 1ull << t;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_CNOT, c, t, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, c, t) | cb; p.x = A(p.i); p.y = A(p.i | tb); return p; },
@@ -736,7 +743,7 @@ struct Shot {
     // exec_array_cz (svm_kernels.inl:255-365)
     __device__ __forceinline__ void array_cz(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), both = (1ull << c) | (1ull << t);
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_CZ, c, t, 0, nullptr, 0);
         } else {
             sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins00(i, c, t) | both; p.x = A(p.i); return p; },
@@ -749,7 +756,7 @@ struct Shot {
     // exec_array_swap (svm_kernels.inl:369-458)
     __device__ __forceinline__ void array_swap(uint32_t a, uint32_t b) {
         const uint64_t n = 1ull << (k - 2), ab = 1ull << a, bb = 1ull << b;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_SWAP, a, b, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, a, b); p.x = A(p.i | ab); p.y = A(p.i | bb); return p; },
@@ -762,7 +769,7 @@ struct Shot {
     // exec_array_multi_cnot (svm_kernels.inl:464-550)
     __device__ __forceinline__ void array_multi_cnot(uint32_t t, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), tb = 1ull << t;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_MCNOT, t, t, mask, nullptr, 0);
         } else {
             sweep<P2>(n,
@@ -792,7 +799,7 @@ struct Shot {
     // exec_array_multi_cz (svm_kernels.inl:558-635)
     __device__ __forceinline__ void array_multi_cz(uint32_t c, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), cb = 1ull << c;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_MCZ, c, c, mask, nullptr, 0);
         } else {
             sweep<P1>(n,
@@ -818,7 +825,7 @@ struct Shot {
     __device__ __forceinline__ void array_h(uint32_t a) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const R s = (R)CGPU_INV_SQRT2;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_H, a, a, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
@@ -834,7 +841,7 @@ struct Shot {
     // apply_phase_waterfall (svm_kernels.inl:764-830)
     __device__ __forceinline__ void phase_sweep(uint32_t a, double re, double im) {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             const double c[2] = {re, im};
             emit(M_PHASE, a, a, 0, c, 2);
         } else {
@@ -859,14 +866,20 @@ struct Shot {
             phase_sweep(a, zr, zi);
         }
     }
-    // Statevector passes of a CTA group with a global-memory statevector larger
-    // than one tile go through the bulk-copy tile engine.
+    // Statevector passes of a one-shot group with a global-memory statevector
+    // larger than one tile go through the bulk-copy tile engine.
     __device__ __forceinline__ bool tiled(uint32_t kk) const {
-        return Grp::kCta && fuse != nullptr && kk > (uint32_t)TileCfg<R>::kBits;
+        return kTiles && fuse != nullptr && kk > (uint32_t)TC::kBits;
     }
     // one run per tile covering the lowest TILE_BITS axes
     __device__ __forceinline__ void set_runs_low() {
         if (Grp::rank() == 0) reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset())[0] = 0;
+    }
+    // run offsets of a tile over axes F (2^(TILE_BITS - r) runs of 2^r amplitudes)
+    __device__ __forceinline__ void set_runs(uint64_t F, uint32_t r) {
+        uint64_t* runoff = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
+        for (int j = Grp::rank(); j < (1 << (TC::kBits - r)); j += Grp::size())
+            runoff[j] = pdep((uint64_t)j << r, F);
     }
 
     // exec_expand / expand_with_phase / exec_expand_{t,t_dag,rot}
@@ -876,15 +889,15 @@ struct Shot {
         int x = with_phase ? f.px(a) : 0;
         const T ph = Cx<R>::make(with_phase ? zr : 1.0, with_phase ? (x ? -zi : zi) : 0.0);
         if (tiled(k)) {
-            if constexpr (Grp::kCta) {
-                constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+            if constexpr (kTiles) {
+                constexpr uint32_t MB = TC::kBits, TN = 1u << MB;
                 set_runs_low();
                 const int tid = Grp::rank(), nthr = Grp::size();
                 cur_site = 1;
                 stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, 0, half, 1, [&](T* buf, uint64_t) {
                     if (with_phase)
                         for (uint32_t l = tid; l < TN; l += nthr) buf[l] = cmul(buf[l], ph);
-                    __syncthreads();
+                    Grp::sync();
                 });
                 moved += (2ull << k) * sizeof(T);
                 bytes += (2ull << k) * sizeof(T);
@@ -917,7 +930,7 @@ struct Shot {
         Frame<NW>::put(f.x, a, out & 1);
         Frame<NW>::put(f.z, a, (out >> 1) & 1);
         if (a >= k) return;
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_U2, a, a, 0, m, 8);
             account(2ull << k);
             return;
@@ -944,7 +957,7 @@ struct Shot {
         Frame<NW>::put(f.z, lo, (out >> 1) & 1);
         Frame<NW>::put(f.x, hi, (out >> 2) & 1);
         Frame<NW>::put(f.z, hi, (out >> 3) & 1);
-        if (Grp::kCta && resolving) {
+        if (kTiles && resolving) {
             emit(M_U4, lo, hi, 0, e, 32);
             account(2ull << k);
             return;
@@ -1058,8 +1071,8 @@ struct Shot {
         double acc[2] = {0.0, 0.0};
         const bool tl = tiled(k);
         if (tl) {
-            if constexpr (Grp::kCta) {
-                constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+            if constexpr (kTiles) {
+                constexpr uint32_t MB = TC::kBits, TN = 1u << MB;
                 set_runs_low();
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint64_t ntiles = 1ull << (k - MB);
@@ -1071,7 +1084,7 @@ struct Shot {
                         acc[1] += q;
                     else
                         acc[0] += q;
-                    __syncthreads();
+                    Grp::sync();
                 });
                 moved += (1ull << k) * sizeof(T);
             }
@@ -1113,11 +1126,11 @@ struct Shot {
         if (b == 1 && pzv) negate_gamma();
         if (b == 1) {
             if (tl) {
-                if constexpr (Grp::kCta) {
-                    constexpr uint32_t MB = TileCfg<R>::kBits, TN = 1u << MB;
+                if constexpr (kTiles) {
+                    constexpr uint32_t MB = TC::kBits, TN = 1u << MB;
                     cur_site = 3;
                     stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, half, 0, 1,
-                                 [&](T*, uint64_t) { __syncthreads(); });
+                                 [&](T*, uint64_t) { Grp::sync(); });
                     moved += (1ull << k) * sizeof(T);
                     bytes += (1ull << k) * sizeof(T);
                 }
@@ -1153,13 +1166,12 @@ struct Shot {
         uint32_t tr = 0, lf = 0;
         uint64_t tC = 0;
         if (tl) {
-            if constexpr (Grp::kCta) {
-                constexpr uint32_t MB = TileCfg<R>::kBits;
+            if constexpr (kTiles) {
+                constexpr uint32_t MB = TC::kBits;
                 const uint64_t F = tile_axes((1ull << t) | fb, tr);
                 tC = ((1ull << k) - 1) & ~F;
                 lf = (uint32_t)__popcll(F & (fb - 1));
-                uint64_t* runoff = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
-                if (Grp::rank() < (1 << (MB - tr))) runoff[Grp::rank()] = pdep((uint64_t)Grp::rank() << tr, F);
+                set_runs(F, tr);
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
                 cur_site = 4;
@@ -1174,7 +1186,7 @@ struct Shot {
                     }
                     acc[0] += qp;
                     acc[1] += qm;
-                    __syncthreads();
+                    Grp::sync();
                 });
                 moved += (1ull << k) * sizeof(T);
             }
@@ -1219,8 +1231,8 @@ struct Shot {
         int m_abs = bx ^ pzv;
         const R s = (R)CGPU_INV_SQRT2;
         if (tl) {
-            if constexpr (Grp::kCta) {
-                constexpr uint32_t MB = TileCfg<R>::kBits;
+            if constexpr (kTiles) {
+                constexpr uint32_t MB = TC::kBits;
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
                 const uint32_t nruns = 1u << (MB - tr);
@@ -1231,7 +1243,7 @@ struct Shot {
                             T x = buf[l], y = buf[l + HN];
                             buf[l] = cscale(bx ? csub(x, y) : cadd(x, y), s);
                         }
-                        __syncthreads();
+                        Grp::sync();
                     } else {
                         // outputs with the fa bit clear read positions the fa-set outputs overwrite
                         for (int pass = 0; pass < 2; ++pass) {
@@ -1241,7 +1253,7 @@ struct Shot {
                                 T x = buf[a0], y = buf[a0 | lfb];
                                 buf[l] = cscale(bx ? csub(x, y) : cadd(x, y), s);
                             }
-                            __syncthreads();
+                            Grp::sync();
                         }
                     }
                 });
@@ -1537,7 +1549,7 @@ struct Shot {
     // contiguous low run, so one tile is 2^(TILE_BITS - r) runs of 2^r
     // consecutive amplitudes.
     __device__ __forceinline__ uint64_t tile_axes(uint64_t uni, uint32_t& r) const {
-        constexpr uint32_t MB = TileCfg<R>::kBits;
+        constexpr uint32_t MB = TC::kBits;
         uint64_t F = uni;
         for (uint32_t a = 0; (uint32_t)__popcll(F) < MB; ++a) F |= 1ull << a;
         r = (uint32_t)__ffsll((long long)~F) - 1;  // count of consecutive low axes in F
@@ -1548,25 +1560,28 @@ struct Shot {
     // tile t covers the run offsets `runoff` (shared table, 2^(TILE_BITS - r)
     // runs of 2^r amplitudes) shifted by pdep(t, C). Loads come from
     // v[load_add + ...], optional stores (the first `store_runs` runs of each
-    // tile) go to v[store_add + ...]. Bulk copies (TMA) run K.stages tiles
-    // ahead; `compute(buf, t)` is called by every thread and must synchronise
-    // the CTA before it returns. Returns false after a barrier timeout.
+    // tile) go to v[store_add + ...]. Bulk copies (TMA) run K.stages - 1
+    // tiles ahead; `compute(buf, t)` is called by every thread of the group
+    // and must synchronise the group before it returns. Returns false after a
+    // barrier timeout.
     uint32_t cur_pc = 0;   // instruction being executed (diagnostics)
     uint32_t cur_site = 0; // which statevector pass is streaming (diagnostics)
     template <class Compute>
     __device__ bool stream_tiles(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add, uint64_t store_add,
                                  uint32_t store_runs, Compute compute) {
-        constexpr uint32_t MB = TileCfg<R>::kBits;
+        constexpr uint32_t MB = TC::kBits;
         constexpr uint32_t TN = 1u << MB;
-        T* bufs = reinterpret_cast<T*>(fuse + kFuseBufOffset);
+        T* bufs = reinterpret_cast<T*>(fuse + TC::kBufOffset);
         uint64_t* bars = reinterpret_cast<uint64_t*>(fuse + fuse_bar_offset());
         const uint32_t nst = K.stages;
         const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
         const uint32_t nruns = 1u << (MB - r);
         const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
-        const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-        // The stage barriers are initialised once per CTA (kernel entry); each
-        // call continues from the phase every stage is in, tracked in
+        // the issuing warp: warp 0 of a CTA group, the shot's own warp otherwise
+        const bool issuer = Grp::kCta ? (threadIdx.x >> 5) == 0 : true;
+        const int lane = threadIdx.x & 31;
+        // The stage barriers are initialised once per group (kernel entry);
+        // each call continues from the phase every stage is in, tracked in
         // *bar_phase identically by every thread.
         uint32_t phase = *bar_phase;
         if (phase >> 31) {
@@ -1575,7 +1590,7 @@ struct Shot {
         }
         // statevector writes made by ordinary stores must be visible to the copy engine
         fence_async_global();
-        __syncthreads();
+        Grp::sync();
         auto issue_load = [&](uint64_t t) {
             const uint32_t st = (uint32_t)(t % nst);
             const uint64_t base = load_add + pdep(t, C);
@@ -1584,7 +1599,7 @@ struct Shot {
             for (uint32_t j = lane; j < nruns; j += 32)
                 bulk_load(bufs + st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[st]);
         };
-        if (warp == 0)
+        if (issuer)
             for (uint64_t t = 0; t < ntiles && t < (uint64_t)(nst - 1); ++t) issue_load(t);
         bool ok_all = true;
         long long waited = 0;
@@ -1596,32 +1611,37 @@ struct Shot {
             const long long w0 = clock64();
             for (uint32_t it = 0; it < (1u << 20) && !ok; ++it) ok = mbar_try_wait(&bars[st], parity);
             waited = clock64() - w0;
-            if (__syncthreads_or(!ok)) {
+            const bool failed = Grp::kCta ? __syncthreads_or(!ok) != 0 : __any_sync(0xffffffffu, !ok) != 0;
+            if (failed) {
                 ok_all = false;
                 break;
             }
             phase ^= 1u << st;
+            // refill the stage that held tile t-1 before computing tile t:
+            // every thread finished tile t-1 (compute ends with a group
+            // barrier) and its store has read the buffer once the bulk group
+            // drains, so nst-1 tiles stay in flight during the compute
+            if (issuer && t + nst - 1 < ntiles) {
+                if (store_runs) bulk_wait_read0();
+                __syncwarp();
+                issue_load(t + nst - 1);
+            }
             T* buf = bufs + st * TN;
             compute(buf, t);
             if (store_runs) {
                 fence_async_shared();
-                __syncthreads();
-                if (warp == 0) {
+                Grp::sync();
+                if (issuer) {
                     const uint64_t base = store_add + pdep(t, C);
                     for (uint32_t j = lane; j < store_runs; j += 32)
                         bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
                     bulk_commit();
                 }
             }
-            if (warp == 0 && t + nst - 1 < ntiles) {
-                if (store_runs) bulk_wait_read1();  // the stage being refilled held tile t-1
-                __syncwarp();
-                issue_load(t + nst - 1);
-            }
         }
         if (!ok_all) {
             // drain (bounded) every load still in flight before the buffers go away
-            if (tid == 0 && atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT) == 0 && K.error_info) {
+            if (Grp::rank() == 0 && atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT) == 0 && K.error_info) {
                 K.error_info[0] = cur_site;
                 K.error_info[1] = cur_pc;
                 K.error_info[2] = t;
@@ -1631,6 +1651,7 @@ struct Shot {
                 K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[t % nst]);
                 K.error_info[7] = (unsigned long long)waited;
             }
+            // loads in flight at the failed wait: tiles t .. t+nst-2
             for (uint64_t q = t; q < ntiles && q < t + nst - 1; ++q) {
                 const uint32_t st = (uint32_t)(q % nst);
                 for (uint32_t it = 0; it < (1u << 20); ++it)
@@ -1640,24 +1661,24 @@ struct Shot {
             phase |= 1u << 31;
             stop = true;
         }
-        if (warp == 0) {
+        if (issuer) {
             bulk_wait_all();
             fence_async_global();
         }
         *bar_phase = phase;
-        __syncthreads();
+        Grp::sync();
         return ok_all;
     }
 
-    // Fused tile sweep starting at `pc` (CTA groups, statevector in global
-    // memory, k > tile bits). Returns the number of instructions consumed, 0
-    // when the opcode at `pc` cannot start a block.
-    __device__ uint32_t fused_block(uint32_t pc, int max_ops) {
-        constexpr uint32_t MB = TileCfg<R>::kBits;
+    // Fused tile sweep starting at `pc` (one-shot groups, statevector in
+    // global memory, k > tile bits), ending before `limit`. Returns the number
+    // of instructions consumed, 0 when the opcode at `pc` cannot start a block.
+    __device__ uint32_t fused_block(uint32_t pc, int max_ops, uint32_t limit) {
+        constexpr uint32_t MB = TC::kBits;
         uint64_t uni = 0;
         int nsweep = 0;
         uint32_t end = pc;
-        for (; end < P.n_instr; ++end) {
+        for (; end < limit; ++end) {
             const uint4 w0 = __ldg(P.instr + 2 * end);
             const uint32_t op = w0.x & 0xffu, x1 = w0.y & 0xffffu, x2 = w0.y >> 16;
             uint64_t m = 0;
@@ -1700,13 +1721,12 @@ struct Shot {
         const uint64_t F = tile_axes(uni, r);
         const uint64_t C = ((k == 64) ? ~0ull : ((1ull << k) - 1)) & ~F;
         uint8_t* lbit = reinterpret_cast<uint8_t*>(fuse + fuse_lbit_offset());
-        uint64_t* runoff = reinterpret_cast<uint64_t*>(fuse + fuse_tables_offset());
         if (Grp::rank() == 0) {
             uint32_t j = 0;
             for (uint32_t a = 0; a < k; ++a)
                 if ((F >> a) & 1u) lbit[a] = (uint8_t)j++;
         }
-        if (Grp::rank() < (1 << (MB - r))) runoff[Grp::rank()] = pdep((uint64_t)Grp::rank() << r, F);
+        set_runs(F, r);
         Grp::sync();
         // resolve the block's frame-dependent choices into micro-ops
         resolving = true;
@@ -1725,8 +1745,8 @@ struct Shot {
                 int e = j;
                 while (e < nm && index_map_kind(mops[e].kind)) ++e;
                 if (e - j >= 2 && rpt <= kMaxRunAmps) {
-                    if (rpt == 16)
-                        apply_index_run<16>(mops, j, e, buf, tid, nthr);
+                    if (kMaxRunAmps >= 16 && rpt == 16)
+                        apply_index_run<(kMaxRunAmps >= 16 ? 16 : 8)>(mops, j, e, buf, tid, nthr);
                     else if (rpt == 8)
                         apply_index_run<8>(mops, j, e, buf, tid, nthr);
                     else
@@ -1735,7 +1755,7 @@ struct Shot {
                     continue;
                 }
                 apply_micro(mops[j], buf, tid, nthr);
-                __syncthreads();
+                Grp::sync();
                 ++j;
             }
         });
@@ -1804,16 +1824,16 @@ struct Shot {
                 }
             }
         }
-        __syncthreads();
+        Grp::sync();
 #pragma unroll
         for (int q = 0; q < RPT; ++q) tile[pos[q]] = v[q];
-        __syncthreads();
+        Grp::sync();
     }
 
     // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes; the
     // arithmetic matches the unfused opcode handlers exactly.
     static __device__ __forceinline__ void apply_micro(const MicroOp& m, T* tile, int tid, int nthr) {
-        constexpr uint32_t MB = TileCfg<R>::kBits;
+        constexpr uint32_t MB = TC::kBits;
         const uint32_t a = m.a, b = m.b;
         const uint32_t ab = 1u << a, bb = 1u << b;
         switch (m.kind) {
@@ -1999,7 +2019,7 @@ struct Shot {
     // a statevector step executed by every thread (fused block or one opcode)
     __device__ __forceinline__ uint32_t run_all(uint32_t pc, bool fuse_on) {
         uint32_t used = 0;
-        if (tiled(k)) used = fused_block(pc, fuse_on ? kMaxMicroOps : 1);
+        if (tiled(k)) used = fused_block(pc, fuse_on ? TC::kMops : 1, P.n_instr);
         if (!used) {
             exec(pc);
             used = 1;
@@ -2068,10 +2088,21 @@ struct Shot {
             run_cta(fuse_on, prof);
         } else {
             const uint32_t end = seg ? K.seg_end : n_instr;
-            for (uint32_t pc = seg ? K.seg_begin : 0; pc < end; ++pc) {
+            const int max_ops = (K.flags & KF_FUSE) ? TC::kMops : 1;
+            for (uint32_t pc = seg ? K.seg_begin : 0; pc < end;) {
                 pc = frame_run(pc, end);
                 if (pc >= end) break;
-                exec(pc);
+                uint32_t used = 0;
+                if constexpr (kTiles) {
+                    // a warp running one shot streams its global statevector
+                    // through the tile engine like a CTA group
+                    if (tiled(k)) used = fused_block(pc, max_ops, end);
+                }
+                if (!used) {
+                    exec(pc);
+                    used = 1;
+                }
+                pc += used;
                 if (stop) break;
             }
         }
@@ -2290,6 +2321,7 @@ struct Shot {
 // Shared memory per warp (G > 0) or per CTA (G = 0):
 //   [interleaved statevectors: 2^peak x S amplitudes, when state_in_smem]
 //   [records: (rec_words + det_words + obs_words) x S u32, interleaved]
+//   [tile-engine scratch (TileCfg), one-shot groups with global statevectors]
 // then, for the whole block: 3 doubles per warp of reduction scratch and a
 // broadcast slot.
 template <int G>
@@ -2318,10 +2350,11 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
     uint32_t* obs = det + (size_t)K.det_words * S;
     unsigned char* fz = K.fuse_bytes ? rbase + state_bytes + rec_bytes : nullptr;
     uint32_t bar_phase = 0;
-    if (Grp::kCta && fz != nullptr) {
-        // tile-engine stage barriers: initialised once, reused by every pass
-        // of every shot this CTA runs
-        if (threadIdx.x == 0) {
+    if (fz != nullptr) {
+        // tile-engine stage barriers of each one-shot group (the CTA, or each
+        // warp): initialised once, reused by every pass of every shot the
+        // group runs
+        if (Grp::rank() == 0) {
             uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW>::fuse_bar_offset());
             for (int st = 0; st < kMaxStages; ++st) mbar_init(&bars[st], 1);
             mbar_fence_init();
@@ -2346,7 +2379,9 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
             base = *bcast;
             __syncthreads();
         } else {
-            if ((threadIdx.x & 31) == 0) base = atomicAdd(K.work_counter, (unsigned long long)S);
+            // a warp whose tile barriers timed out takes no further shots
+            if ((threadIdx.x & 31) == 0)
+                base = (bar_phase >> 31) ? ~0ull : atomicAdd(K.work_counter, (unsigned long long)S);
             base = __shfl_sync(0xffffffffu, base, 0);
         }
         if (base >= n_items) break;

@@ -222,19 +222,20 @@ def test_record_probabilities_match_oracle():
     np.testing.assert_allclose(lp[reach], f["log_prob"][reach], atol=1e-10)
 
 
-@pytest.mark.parametrize("group", [256, 512])
+@pytest.mark.parametrize("group", [32, 256, 512])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_fused_tile_sweeps_match_unfused(precision, group):
     # k = 16 with the reference's U2 / U4 / MULTI nodes: fused tile sweeps
     # perform each amplitude's arithmetic in the same order as one sweep per
-    # opcode, so the two executors agree bit for bit (256-thread CTAs stream
-    # through three tile buffers, 512-thread CTAs through four)
+    # opcode, so the two executors agree bit for bit (a warp per shot streams
+    # 4 KiB tiles through three buffers, 256-thread CTAs 32 KiB tiles through
+    # three, 512-thread CTAs through four)
     prog, d = load_case(os.path.join(os.path.dirname(__file__), "golden", "fuzz_k16.npz"))
     fm = d["forced_meas_in"]
     faults, ros = unflatten(d)
     n = fm.shape[0]
     kw = dict(precision=precision, forced_meas=fm, faults=faults, readout_faults=ros, trace=True,
-              dump_shots=n, group_threads=group)  # fusion is a feature of CTA groups (tile engine)
+              dump_shots=n, group_threads=group)  # fusion is a feature of one-shot groups (tile engine)
     a = cb.run(prog, n, 0, fusion=True, **kw)
     b = cb.run(prog, n, 0, fusion=False, **kw)
     assert a["fused"] and not b["fused"]
