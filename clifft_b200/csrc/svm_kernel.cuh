@@ -210,6 +210,17 @@ __device__ __forceinline__ T cmul(T a, T b) {
     r.y = rn_fma(a.x, b.y, rn_mul(a.y, b.x));
     return r;
 }
+// acc + a b, the sum step of a matrix row. FP64 rounds the product and then
+// the sum (the reference's complex<double> arithmetic, which the oracle
+// reproduces bit for bit); FP32 folds each part into two fused multiply-adds,
+// which halves the instructions of the dense U2 / U4 nodes and rounds less.
+__device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) { return cadd(acc, cmul(a, b)); }
+__device__ __forceinline__ float2 cmac(float2 acc, float2 a, float2 b) {
+    float2 r;
+    r.x = rn_fma(a.x, b.x, rn_fma(-a.y, b.y, acc.x));
+    r.y = rn_fma(a.x, b.y, rn_fma(a.y, b.x, acc.y));
+    return r;
+}
 template <typename T, typename S>
 __device__ __forceinline__ T cscale(T a, S s) {
     T r;
@@ -310,6 +321,15 @@ __device__ __forceinline__ uint64_t ins00(uint64_t v, uint32_t a, uint32_t b) {
     uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
     return ins0(ins0(v, lo), hi);
 }
+// the same on tile-local (32-bit) indices
+__device__ __forceinline__ uint32_t ins0_32(uint32_t v, uint32_t pos) {
+    const uint32_t m = (1u << pos) - 1u;
+    return (v & m) | ((v & ~m) << 1);
+}
+__device__ __forceinline__ uint32_t ins00_32(uint32_t v, uint32_t a, uint32_t b) {
+    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    return ins0_32(ins0_32(v, lo), hi);
+}
 
 // Frame words in registers. Axes are < 64 * NW by validation.
 template <int NW>
@@ -407,14 +427,14 @@ constexpr int kMaxStages = 4;      // tile buffers (tiles in flight) per shot gr
 constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 // Tile-engine geometry of a one-shot group. A CTA streams 32 KiB tiles and
 // fuses up to 24 opcodes per pass; a warp running one shot streams 4 KiB
-// tiles and fuses up to 8, so that three buffers per warp leave room for
-// three 4-warp CTAs per SM. Scratch layout of one group: [kMaxStages
+// tiles through two buffers and fuses up to 16, which leaves room for four
+// 4-warp CTAs per SM (the register limit). Scratch layout of one group: [kMaxStages
 // mbarriers][micro-ops][64 run offsets][64-byte axis -> local bit table]
 // [stages tile buffers, 128-B aligned].
 template <typename R, bool CTA>
 struct TileCfg {
     static constexpr int kBits = CTA ? (sizeof(R) == 4 ? 12 : 11) : (sizeof(R) == 4 ? 9 : 8);
-    static constexpr int kMops = CTA ? 24 : 8;
+    static constexpr int kMops = CTA ? 24 : 16;
     static constexpr uint32_t kBarOffset = 0;
     static constexpr uint32_t kMopsOffset = kMaxStages * 8u;
     static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MicroOp);
@@ -714,16 +734,18 @@ struct Shot {
     static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return TC::kLbitOffset; }
     __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
                                          int nc) {
+        MicroOp* m = reinterpret_cast<MicroOp*>(fuse + fuse_mops_offset()) + n_mops;
         if (Grp::rank() == 0) {
-            MicroOp* m = reinterpret_cast<MicroOp*>(fuse + fuse_mops_offset()) + n_mops;
             m->kind = kind;
             m->a = local_bit(a);
             m->b = local_bit(b);
             uint32_t lm = 0;
             for (uint64_t w = mask; w; w &= w - 1) lm |= 1u << local_bit((uint32_t)__ffsll((long long)w) - 1);
             m->mask = lm;
-            for (int j = 0; j < nc; ++j) m->c[j] = c[j];
         }
+        // coefficients (up to 32 doubles of a U4 node) copied one per thread:
+        // one global-load latency instead of a serial chain of them
+        for (int j = Grp::rank(); j < nc; j += Grp::size()) m->c[j] = c[j];
         n_mops++;
     }
 
@@ -940,8 +962,8 @@ struct Shot {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
                   [&](const P2& p) {
-                      A(p.i) = cadd(cmul(m00, p.x), cmul(m01, p.y));
-                      A(p.i | ab) = cadd(cmul(m10, p.x), cmul(m11, p.y));
+                      A(p.i) = cmac(cmul(m00, p.x), m01, p.y);
+                      A(p.i | ab) = cmac(cmul(m10, p.x), m11, p.y);
                   });
         Grp::sync();
         account(2ull << k);
@@ -981,9 +1003,9 @@ struct Shot {
 #pragma unroll
                       for (int r = 0; r < 4; ++r) {
                           T acc = cmul(m[r * 4 + 0], p.x0);
-                          acc = cadd(acc, cmul(m[r * 4 + 1], p.x1));
-                          acc = cadd(acc, cmul(m[r * 4 + 2], p.x2));
-                          acc = cadd(acc, cmul(m[r * 4 + 3], p.x3));
+                          acc = cmac(acc, m[r * 4 + 1], p.x1);
+                          acc = cmac(acc, m[r * 4 + 2], p.x2);
+                          acc = cmac(acc, m[r * 4 + 3], p.x3);
                           y[r] = acc;
                       }
                       A(p.i) = y[0];
@@ -1248,7 +1270,7 @@ struct Shot {
                         // outputs with the fa bit clear read positions the fa-set outputs overwrite
                         for (int pass = 0; pass < 2; ++pass) {
                             for (uint32_t j = tid; j < HN / 2; j += nthr) {
-                                uint32_t l = (uint32_t)ins0(j, lf) | (pass ? lfb : 0u);
+                                uint32_t l = ins0_32(j, lf) | (pass ? lfb : 0u);
                                 uint32_t a0 = pass ? ((l & ~lfb) | HN) : l;
                                 T x = buf[a0], y = buf[a0 | lfb];
                                 buf[l] = cscale(bx ? csub(x, y) : cadd(x, y), s);
@@ -1839,7 +1861,7 @@ struct Shot {
         switch (m.kind) {
             case M_CNOT:
                 for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t b0 = (uint32_t)ins00(i, a, b) | ab;
+                    uint32_t b0 = ins00_32(i, a, b) | ab;
                     T x = tile[b0];
                     tile[b0] = tile[b0 | bb];
                     tile[b0 | bb] = x;
@@ -1847,13 +1869,13 @@ struct Shot {
                 break;
             case M_CZ:
                 for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t idx = (uint32_t)ins00(i, a, b) | ab | bb;
+                    uint32_t idx = ins00_32(i, a, b) | ab | bb;
                     tile[idx] = cneg(tile[idx]);
                 }
                 break;
             case M_SWAP:
                 for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t base = (uint32_t)ins00(i, a, b);
+                    uint32_t base = ins00_32(i, a, b);
                     T x = tile[base | ab];
                     tile[base | ab] = tile[base | bb];
                     tile[base | bb] = x;
@@ -1861,7 +1883,7 @@ struct Shot {
                 break;
             case M_MCNOT:
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    uint32_t i0 = ins0_32(i, a);
                     if (__popc(i0 & m.mask) & 1) {
                         T x = tile[i0];
                         tile[i0] = tile[i0 | ab];
@@ -1871,14 +1893,14 @@ struct Shot {
                 break;
             case M_MCZ:
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = (uint32_t)ins0(i, a) | ab;
+                    uint32_t i0 = ins0_32(i, a) | ab;
                     if (__popc(i0 & m.mask) & 1) tile[i0] = cneg(tile[i0]);
                 }
                 break;
             case M_H: {
                 const R s = (R)CGPU_INV_SQRT2;
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    uint32_t i0 = ins0_32(i, a);
                     T x = tile[i0], y = tile[i0 | ab];
                     tile[i0] = cscale(cadd(x, y), s);
                     tile[i0 | ab] = cscale(csub(x, y), s);
@@ -1888,7 +1910,7 @@ struct Shot {
             case M_PHASE: {
                 const T ph = Cx<R>::make(m.c[0], m.c[1]);
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t idx = (uint32_t)ins0(i, a) | ab;
+                    uint32_t idx = ins0_32(i, a) | ab;
                     tile[idx] = cmul(tile[idx], ph);
                 }
                 break;
@@ -1897,25 +1919,38 @@ struct Shot {
                 const T m00 = Cx<R>::make(m.c[0], m.c[1]), m01 = Cx<R>::make(m.c[2], m.c[3]);
                 const T m10 = Cx<R>::make(m.c[4], m.c[5]), m11 = Cx<R>::make(m.c[6], m.c[7]);
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = (uint32_t)ins0(i, a);
+                    uint32_t i0 = ins0_32(i, a);
                     T x = tile[i0], y = tile[i0 | ab];
-                    tile[i0] = cadd(cmul(m00, x), cmul(m01, y));
-                    tile[i0 | ab] = cadd(cmul(m10, x), cmul(m11, y));
+                    tile[i0] = cmac(cmul(m00, x), m01, y);
+                    tile[i0 | ab] = cmac(cmul(m10, x), m11, y);
                 }
                 break;
             }
             case M_U4: {
+                // FP32: the 16 coefficients converted once and held in registers;
+                // FP64 reads them from shared memory (its registers are spoken for)
+                constexpr bool kHoist = sizeof(R) == 4;
+                T cm[kHoist ? 16 : 1];
+                if constexpr (kHoist) {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) cm[j] = Cx<R>::make(m.c[2 * j], m.c[2 * j + 1]);
+                }
+                auto coef = [&](int j) -> T {
+                    if constexpr (kHoist)
+                        return cm[j];
+                    else
+                        return Cx<R>::make(m.c[2 * j], m.c[2 * j + 1]);
+                };
                 for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t q = (uint32_t)ins00(i, a, b);
+                    uint32_t q = ins00_32(i, a, b);
                     T x0 = tile[q], x1 = tile[q | ab], x2 = tile[q | bb], x3 = tile[q | ab | bb];
                     T y[4];
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
-                        const double* row = m.c + r * 8;
-                        T acc = cmul(Cx<R>::make(row[0], row[1]), x0);
-                        acc = cadd(acc, cmul(Cx<R>::make(row[2], row[3]), x1));
-                        acc = cadd(acc, cmul(Cx<R>::make(row[4], row[5]), x2));
-                        acc = cadd(acc, cmul(Cx<R>::make(row[6], row[7]), x3));
+                        T acc = cmul(coef(4 * r), x0);
+                        acc = cmac(acc, coef(4 * r + 1), x1);
+                        acc = cmac(acc, coef(4 * r + 2), x2);
+                        acc = cmac(acc, coef(4 * r + 3), x3);
                         y[r] = acc;
                     }
                     tile[q] = y[0];
