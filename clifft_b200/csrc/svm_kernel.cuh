@@ -1613,21 +1613,29 @@ struct Shot {
         // statevector writes made by ordinary stores must be visible to the copy engine
         fence_async_global();
         Grp::sync();
-        auto issue_load = [&](uint64_t t) {
-            const uint32_t st = (uint32_t)(t % nst);
-            const uint64_t base = load_add + pdep(t, C);
-            if (lane == 0) mbar_expect_tx(&bars[st], TN * (uint32_t)sizeof(T));
+        // Tile bases and stages advance by running counters (a tile costs a
+        // few hundred instructions at 4 KiB, so no division or bit-deposit
+        // loop per tile): pdep(t + 1, C) = ((pdep(t, C) | ~C) + 1) & C.
+        auto next_base = [C](uint64_t b) { return ((b | ~C) + 1) & C; };
+        uint64_t issue_base = 0;  // pdep(next tile to load, C)
+        uint32_t issue_st = 0;    // its stage
+        auto issue_next = [&]() {
+            if (lane == 0) mbar_expect_tx(&bars[issue_st], TN * (uint32_t)sizeof(T));
             __syncwarp();
+            const uint64_t base = load_add + issue_base;
             for (uint32_t j = lane; j < nruns; j += 32)
-                bulk_load(bufs + st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[st]);
+                bulk_load(bufs + issue_st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[issue_st]);
+            issue_base = next_base(issue_base);
+            issue_st = issue_st + 1 == nst ? 0 : issue_st + 1;
         };
         if (issuer)
-            for (uint64_t t = 0; t < ntiles && t < (uint64_t)(nst - 1); ++t) issue_load(t);
+            for (uint64_t t = 0; t < ntiles && t < (uint64_t)(nst - 1); ++t) issue_next();
         bool ok_all = true;
         long long waited = 0;
         uint64_t t = 0;
-        for (; t < ntiles; ++t) {
-            const uint32_t st = (uint32_t)(t % nst);
+        uint32_t st = 0;      // stage of tile t
+        uint64_t tbase = 0;   // pdep(t, C)
+        for (; t < ntiles; ++t, tbase = next_base(tbase), st = st + 1 == nst ? 0 : st + 1) {
             const uint32_t parity = (phase >> st) & 1u;
             uint32_t ok = 0;
             const long long w0 = clock64();
@@ -1646,7 +1654,7 @@ struct Shot {
             if (issuer && t + nst - 1 < ntiles) {
                 if (store_runs) bulk_wait_read0();
                 __syncwarp();
-                issue_load(t + nst - 1);
+                issue_next();  // tile t + nst - 1
             }
             T* buf = bufs + st * TN;
             compute(buf, t);
@@ -1654,7 +1662,7 @@ struct Shot {
                 fence_async_shared();
                 Grp::sync();
                 if (issuer) {
-                    const uint64_t base = store_add + pdep(t, C);
+                    const uint64_t base = store_add + tbase;
                     for (uint32_t j = lane; j < store_runs; j += 32)
                         bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
                     bulk_commit();
@@ -1670,15 +1678,15 @@ struct Shot {
                 K.error_info[3] = ntiles;
                 K.error_info[4] = r;
                 K.error_info[5] = k;
-                K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[t % nst]);
+                K.error_info[6] = *reinterpret_cast<volatile unsigned long long*>(&bars[st]);
                 K.error_info[7] = (unsigned long long)waited;
             }
             // loads in flight at the failed wait: tiles t .. t+nst-2
             for (uint64_t q = t; q < ntiles && q < t + nst - 1; ++q) {
-                const uint32_t st = (uint32_t)(q % nst);
+                const uint32_t sq = (uint32_t)(q % nst);
                 for (uint32_t it = 0; it < (1u << 20); ++it)
-                    if (mbar_try_wait(&bars[st], (phase >> st) & 1u)) break;
-                phase ^= 1u << st;
+                    if (mbar_try_wait(&bars[sq], (phase >> sq) & 1u)) break;
+                phase ^= 1u << sq;
             }
             phase |= 1u << 31;
             stop = true;
