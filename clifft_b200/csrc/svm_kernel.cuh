@@ -1652,20 +1652,36 @@ struct Shot {
             // barrier) and its store has read the buffer once the bulk group
             // drains, so nst-1 tiles stay in flight during the compute
             if (issuer && t + nst - 1 < ntiles) {
-                if (store_runs) bulk_wait_read0();
+                if (Grp::kCta && store_runs) bulk_wait_read0();
                 __syncwarp();
                 issue_next();  // tile t + nst - 1
             }
             T* buf = bufs + st * TN;
             compute(buf, t);
             if (store_runs) {
-                fence_async_shared();
-                Grp::sync();
-                if (issuer) {
-                    const uint64_t base = store_add + tbase;
-                    for (uint32_t j = lane; j < store_runs; j += 32)
-                        bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
-                    bulk_commit();
+                const uint64_t base = store_add + tbase;
+                if constexpr (Grp::kCta) {
+                    // bulk stores issued by warp 0 (32 KiB tiles)
+                    fence_async_shared();
+                    Grp::sync();
+                    if (issuer) {
+                        for (uint32_t j = lane; j < store_runs; j += 32)
+                            bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
+                        bulk_commit();
+                    }
+                } else {
+                    // a warp writes its 4 KiB tile back with 16-byte stores
+                    // from every lane: a bulk store per tile costs its issuing
+                    // warp more (queueing behind the SM's other copies, then
+                    // a wait before the buffer is refilled) than it saves
+                    const uint32_t clog = r + (sizeof(T) == 8 ? 0u : 1u) - 1u;  // 16-B chunks per run, log2
+                    const uint32_t nchunks = store_runs << clog;
+                    for (uint32_t c = lane; c < nchunks; c += 32) {
+                        const uint32_t j = c >> clog, w = c & ((1u << clog) - 1u);
+                        const uint4 val = reinterpret_cast<const uint4*>(buf + (j << r))[w];
+                        reinterpret_cast<uint4*>(v + base + runoff[j])[w] = val;
+                    }
+                    __syncwarp();
                 }
             }
         }
