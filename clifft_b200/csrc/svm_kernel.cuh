@@ -484,15 +484,15 @@ __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Scalar state the control warp of a CTA group hands to the worker warps
 // before a statevector sweep.
@@ -1591,6 +1591,9 @@ struct Shot {
     template <class Compute>
     __device__ bool stream_tiles(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add, uint64_t store_add,
                                  uint32_t store_runs, Compute compute) {
+        if constexpr (!Grp::kCta) {
+            return stream_tiles_warp(ntiles, C, r, load_add, store_add, store_runs, compute);
+        }
         constexpr uint32_t MB = TC::kBits;
         constexpr uint32_t TN = 1u << MB;
         T* bufs = reinterpret_cast<T*>(fuse + TC::kBufOffset);
@@ -1714,6 +1717,57 @@ struct Shot {
         *bar_phase = phase;
         Grp::sync();
         return ok_all;
+    }
+
+    // The same pass for a warp running one shot: two 4 KiB buffers filled by
+    // 16-byte asynchronous copies from every lane (cp.async, waited for per
+    // lane, then a warp barrier) and written back with 16-byte stores. Bulk
+    // copies of 4 KiB tiles queue behind the SM's other copies; lane copies
+    // keep the warp's loads in the load/store path. Nothing here spins: a
+    // copy group always completes.
+    template <class Compute>
+    __device__ bool stream_tiles_warp(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add,
+                                      uint64_t store_add, uint32_t store_runs, Compute compute) {
+        constexpr uint32_t TN = 1u << TC::kBits;
+        T* bufs = reinterpret_cast<T*>(fuse + TC::kBufOffset);
+        const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
+        const uint32_t lane = threadIdx.x & 31;
+        const uint32_t clog = r + (sizeof(T) == 8 ? 0u : 1u) - 1u;  // 16-B chunks per run, log2
+        const uint32_t wmask = (1u << clog) - 1u;
+        const uint32_t load_chunks = (1u << (TC::kBits - r)) << clog;
+        const uint32_t store_chunks = store_runs << clog;
+        auto next_base = [C](uint64_t b) { return ((b | ~C) + 1) & C; };
+        auto load_tile = [&](T* dst, uint64_t tb) {
+            const uint64_t base = load_add + tb;
+            for (uint32_t c = lane; c < load_chunks; c += 32) {
+                const uint32_t j = c >> clog, w = c & wmask;
+                cp_async16(reinterpret_cast<uint4*>(dst + (j << r)) + w, reinterpret_cast<const uint4*>(v + base + runoff[j]) + w);
+            }
+            cp_async_commit();
+        };
+        // the run table was written by other lanes; statevector writes of
+        // the previous pass must be visible before the copies read them
+        __syncwarp();
+        load_tile(bufs, 0);
+        uint64_t tbase = 0;
+        for (uint64_t t = 0; t < ntiles; ++t) {
+            T* buf = bufs + (t & 1u) * TN;
+            cp_async_wait<0>();
+            __syncwarp();
+            const uint64_t nb = next_base(tbase);
+            if (t + 1 < ntiles) load_tile(bufs + ((t + 1) & 1u) * TN, nb);
+            compute(buf, t);
+            if (store_runs) {
+                const uint64_t base = store_add + tbase;
+                for (uint32_t c = lane; c < store_chunks; c += 32) {
+                    const uint32_t j = c >> clog, w = c & wmask;
+                    reinterpret_cast<uint4*>(v + base + runoff[j])[w] = reinterpret_cast<const uint4*>(buf + (j << r))[w];
+                }
+                __syncwarp();
+            }
+            tbase = nb;
+        }
+        return true;
     }
 
     // Fused tile sweep starting at `pc` (one-shot groups, statevector in
