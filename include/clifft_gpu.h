@@ -127,7 +127,8 @@ typedef struct clifft_gpu_outputs {
     uint32_t state_in_smem;    /* 1 if the statevectors lived in shared memory */
     uint32_t fused;            /* 1 if fused tile sweeps were enabled */
     uint64_t phase_cycles[5];  /* CLIFFT_GPU_PROFILE: SM cycles in fused blocks, measurements, expansions,
-                                  unfused array sweeps, other opcodes (summed over shot groups) */
+                                  unfused array sweeps, other opcodes (summed over CTA shot groups;
+                                  zero when shots run on warps) */
 } clifft_gpu_outputs;
 
 /* Upload + validate a program. *out receives an opaque handle. */
