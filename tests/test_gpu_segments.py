@@ -42,3 +42,30 @@ def test_segmented_fp64_matches_oracle_streams():
     assert np.array_equal(g["survived"].astype(bool), keep)
     gm = cb.api._unpack(g["meas_words"], prog.num_measurements)
     assert np.array_equal(gm[keep], o["meas"][keep])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_segmented_warp_tile_run_equals_one_launch(precision):
+    # peak k = 13: one warp per shot with a global statevector, streamed
+    # through the warp's 4 KiB tiles; shots alive at a cut carry 2^k
+    # amplitudes between segment launches
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from _programs import random_program
+    prog = random_program(8, n=18, length=400, max_k=13, postselect=True, expand_bias=0.2)
+    assert prog.peak_rank == 13
+    shots = 12_000  # > 4 resident waves of 16 warps on every SM
+    seg = cb.run(prog, shots, 19, precision=precision, survivors=True, group_threads=32)
+    one = cb.run(prog, shots, 19, precision=precision, survivors=True, group_threads=32, segments=False)
+    assert seg["state_in_smem"] == 0 and seg["fused"]
+    assert seg["kernel_launches"] > one["kernel_launches"]
+    for key in ("meas_words", "det_words", "obs_words", "survived", "exp_vals"):
+        assert np.array_equal(seg[key], one[key]), key
+    assert seg["passed_shots"] == one["passed_shots"] > 0
+    if precision == "fp64":
+        n = 300  # per-shot Philox streams: the first shots of the run equal an oracle run of n shots
+        o = O.run(prog, n, seed=19, rng=O.RNG_PHILOX)
+        keep = o["discarded"] == 0
+        assert np.array_equal(seg["survived"][:n].astype(bool), keep)
+        gm = cb.api._unpack(seg["meas_words"][:n], prog.num_measurements)
+        assert np.array_equal(gm[keep], o["meas"][keep])
