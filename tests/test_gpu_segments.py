@@ -52,7 +52,7 @@ def test_segmented_warp_tile_run_equals_one_launch(precision):
     import sys
     sys.path.insert(0, os.path.dirname(__file__))
     from _programs import random_program
-    prog = random_program(8, n=18, length=400, max_k=13, postselect=True, expand_bias=0.2)
+    prog = random_program(21, n=18, length=400, max_k=13, postselect=True, expand_bias=0.2)
     assert prog.peak_rank == 13
     shots = 12_000  # > 4 resident waves of 16 warps on every SM
     seg = cb.run(prog, shots, 19, precision=precision, survivors=True, group_threads=32)
