@@ -540,8 +540,8 @@ struct Shot {
     unsigned long long bytes;  // algorithmic statevector bytes moved by this shot
     const uint8_t* forced;
     double* meas_prob;
-    // fused-sweep state (CTA groups only)
-    unsigned char* fuse;       // shared scratch: 2 tile buffers, micro-ops, index tables
+    // fused-sweep state (one-shot groups with a global statevector)
+    unsigned char* fuse;       // shared scratch: stage barriers, micro-ops, index tables, tile buffers
     uint32_t* bar_phase;       // CTA groups: bit st = parity of the phase stage st's barrier is in;
                                // bit 31 set once a wait timed out (the barriers are then unusable)
     bool resolving;            // true while a fused block's opcodes emit micro-ops
