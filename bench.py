@@ -245,13 +245,15 @@ def cpu_baseline(name):
     prog = load_program(name)
     cores = len(os.sched_getaffinity(0))
     if O.ref_available():
+        O.ref_select_native()
         modes = ref_modes(prog, cores, 6.0)
         best = max(modes, key=lambda m: m[1])
         t1 = O.ref_time_sample(prog, 2, 5, 1, bool(prog.has_postselection), 1)
         desc = "; ".join(f"{m}: {n} shots in {t:.1f} s = {v:.3g}/s" for m, v, n, t in modes)
         return {"value": best[1], "unit": "shots/s", "cores": cores, "kind": "reference",
                 "sample": f"{name} program, reference clifft::sample built from its sources (oracle/_ref, "
-                          f"dispatch {O.ref_backend()}); best of [{desc}]; 1 core: {2 / t1:.3g}/s"}
+                          f"{O.ref_build_kind()} build, dispatch {O.ref_backend()}); best of [{desc}]; "
+                          f"1 core: {2 / t1:.3g}/s"}
     n = 2
     t0 = time.perf_counter()
     O.run(prog, n, seed=3, rng=O.RNG_XOSHIRO)
@@ -268,6 +270,7 @@ def reference_arm(args, config):
         print(json.dumps({"impl": "reference", "unavailable":
                           "reference executor (oracle/_ref) not built on this machine"}))
         return
+    O.ref_select_native()
     # the faster of the reference's two parallel modes on a short probe
     modes = ref_modes(prog, cores, 2.0)
     mode = max(modes, key=lambda m: m[1])[0]
@@ -285,7 +288,7 @@ def reference_arm(args, config):
             "cpu_baseline": {"value": val, "unit": "shots/s", "cores": cores, "kind": "reference",
                              "sample": f"{per_step} shots per step of the {HEADLINE} program, {mode} "
                                        f"({thr} threads x OpenMP team {omp}), reference clifft::sample "
-                                       f"(oracle/_ref)"},
+                                       f"(oracle/_ref, {O.ref_build_kind()} build)"},
             "e2e": {"value": val, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

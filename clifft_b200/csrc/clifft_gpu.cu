@@ -812,6 +812,23 @@ struct DeviceFaults {
     const uint32_t* ro_end = nullptr;
 };
 
+// Message for the first device-side error code a launch recorded; `info`
+// points at the launch's eight words of timeout diagnostics.
+std::string device_error_message(int dev_err, const unsigned long long* info) {
+    std::string msg = dev_err == DEV_ERR_ZERO_NORM    ? "active measurement on a zero-norm state"
+                      : dev_err == DEV_ERR_TIMEOUT    ? "a bounded wait on a bulk-copy barrier timed out"
+                      : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
+                                                      : "unknown device error " + std::to_string(dev_err);
+    if (dev_err == DEV_ERR_TIMEOUT) {
+        const unsigned long long* e = info;
+        msg += " (pass " + std::to_string(e[0]) + ", instruction " + std::to_string(e[1]) + ", tile " +
+               std::to_string(e[2]) + "/" + std::to_string(e[3]) + ", run log2 " + std::to_string(e[4]) + ", k " +
+               std::to_string(e[5]) + ", barrier word " + std::to_string(e[6]) + ", waited " +
+               std::to_string(e[7]) + " cycles)";
+    }
+    return msg;
+}
+
 // clifft_gpu_sample; `dfaults` non-null when the forced-fault lists live on
 // the device (the outputs follow args->flags as usual).
 void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, clifft_gpu_outputs* out,
@@ -1106,20 +1123,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         for (uint64_t s = 0; s < shots && !hpz.empty(); ++s)
             for (uint32_t w = 0; w < nwo; ++w) out->final_pz[s * nwo + w] = hpz[s * nwt + w];
         const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
-        if (dev_err != 0) {
-            std::string msg = dev_err == DEV_ERR_ZERO_NORM    ? "active measurement on a zero-norm state"
-                              : dev_err == DEV_ERR_TIMEOUT    ? "a bounded wait on a bulk-copy barrier timed out"
-                              : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
-                                                              : "unknown device error";
-            if (dev_err == DEV_ERR_TIMEOUT) {
-                const unsigned long long* e = hs.data() + scratch_words - 8;
-                msg += " (pass " + std::to_string(e[0]) + ", instruction " + std::to_string(e[1]) + ", tile " +
-                       std::to_string(e[2]) + "/" + std::to_string(e[3]) + ", run log2 " + std::to_string(e[4]) +
-                       ", k " + std::to_string(e[5]) + ", barrier word " + std::to_string(e[6]) +
-                       ", waited " + std::to_string(e[7]) + " cycles)";
-            }
-            throw ApiError(CLIFFT_GPU_EDEVICE, msg);
-        }
+        if (dev_err != 0) throw ApiError(CLIFFT_GPU_EDEVICE, device_error_message(dev_err, hs.data() + scratch_words - 8));
         out->passed_shots = hs[2];
         out->logical_errors = hs[3];
         out->dust_clamps = hs[4];
@@ -1273,10 +1277,7 @@ int clifft_gpu_sample_noalloc(clifft_gpu_program* prog, const clifft_gpu_sample_
         CUDA_OK(cudaMemcpyAsync(hs, scratch, words * 8, cudaMemcpyDeviceToHost, st));
         CUDA_OK(cudaStreamSynchronize(st));
         const int dev_err = static_cast<int>(hs[1] & 0xffffffffu);
-        if (dev_err != 0)
-            throw ApiError(CLIFFT_GPU_EDEVICE, dev_err == DEV_ERR_ZERO_NORM    ? "active measurement on a zero-norm state"
-                                               : dev_err == DEV_ERR_BAD_OPCODE ? "device reported an invalid opcode"
-                                                                               : "unknown device error");
+        if (dev_err != 0) throw ApiError(CLIFFT_GPU_EDEVICE, device_error_message(dev_err, hs + words - 8));
         out->passed_shots = hs[2];
         out->logical_errors = hs[3];
         out->dust_clamps = hs[4];

@@ -9,7 +9,10 @@ baseline, never by the product package.
   * `ref_*` functions  -> oracle/_ref/libclifft_ref.so, the reference's own
                           executor and bytecode passes built from its sources
                           by oracle/build_ref.sh (present only where the
-                          reference tree was available at build time).
+                          reference tree was available at build time);
+                          `ref_select_native()` switches the timing calls to
+                          the -march=native build of the same sources when
+                          this host can run it.
 """
 
 from __future__ import annotations
@@ -24,6 +27,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libsvm_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libclifft_ref.so")
+REF_NATIVE_SO = os.path.join(HERE, "_ref", "libclifft_ref_native.so")
 
 RNG_XOSHIRO = 0
 RNG_PHILOX = 1
@@ -77,12 +81,45 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+_ref_path = REF_SO
+
+
+def ref_select_native() -> bool:
+    """Use the -march=native build for every later ref_* call if it exists
+    and a child process can run a small sample with it (a host without the
+    build host's instruction set dies of SIGILL there, not here). Returns
+    whether the native build is now in use. Call before the first ref_* call."""
+    global _ref_path
+    if _ref is not None or not os.path.exists(REF_NATIVE_SO):
+        return _ref_path == REF_NATIVE_SO
+    probe = ("import sys; sys.path.insert(0, %r); sys.path.insert(0, %r)\n"
+             "from oracle import pyoracle as O\n"
+             "from clifft_b200.program import OP, Program, instr, p_u32x2\n"
+             "import numpy as np\n"
+             "code = [instr(OP['EXPAND'], 0), instr(OP['EXPAND_T'], 1), instr(OP['ARRAY_H'], 0),\n"
+             "        instr(OP['ARRAY_CNOT'], 0, 1), instr(OP['MEAS_ACTIVE_DIAGONAL'], 1, 0, 0, p_u32x2(0, 0))]\n"
+             "p = Program(num_qubits=2, peak_rank=2, num_measurements=1, total_meas_slots=1,\n"
+             "            instructions=np.frombuffer(b''.join(code), np.uint8).reshape(-1, 32))\n"
+             "O._ref_path = O.REF_NATIVE_SO\n"
+             "O.ref_sample(p, 64, 1); O.ref_time_sample(p, 8, 1, 2, False, 1)\n") % (
+        os.path.dirname(HERE), HERE)
+    import sys
+    ok = subprocess.run([sys.executable, "-c", probe], capture_output=True, timeout=120).returncode == 0
+    if ok:
+        _ref_path = REF_NATIVE_SO
+    return ok
+
+
+def ref_build_kind() -> str:
+    return "native" if _ref_path == REF_NATIVE_SO else "generic"
+
+
 def ref_lib():
     global _ref
     if _ref is None:
         if not ref_available():
             raise FileNotFoundError(f"reference harness not built: {REF_SO}")
-        lib = ctypes.CDLL(REF_SO)
+        lib = ctypes.CDLL(_ref_path)
         lib.ref_last_error.restype = ctypes.c_char_p
         lib.ref_svm_backend.restype = ctypes.c_char_p
         lib.ref_sample.restype = ctypes.c_int

@@ -40,15 +40,17 @@ def _fixture(name):
     return load_case(os.path.join(GOLD, f"{name}.npz"))
 
 
-def _call(entry, prog, shots, seed, precision, flags, forced=None):
+def _call(entry, prog, shots, seed, precision, flags, forced=None, stream=None, device=0):
     """One call of `entry` ("clifft_gpu_sample" or "clifft_gpu_sample_noalloc")
-    with device buffers for every input and output."""
+    with device buffers for every input and output, on `stream` (a
+    torch.cuda.Stream; None = the legacy default stream) of cuda:`device`."""
     torch = _torch()
     from clifft_b200 import _native as N
     from clifft_b200 import api as cb
 
+    torch.cuda.set_device(device)
     dp = cb.load(prog)
-    dev = torch.device("cuda")
+    dev = torch.device("cuda", device)
     mw, dw, ow = (prog.num_measurements + 63) // 64, (prog.num_detectors + 63) // 64, \
         (prog.num_observables + 63) // 64
     bufs = {
@@ -62,6 +64,7 @@ def _call(entry, prog, shots, seed, precision, flags, forced=None):
     a.shots, a.seed, a.first_shot = shots, seed, 0
     a.precision = N.CLIFFT_GPU_FP64 if precision == "fp64" else N.CLIFFT_GPU_FP32
     a.flags = flags | N.CLIFFT_GPU_DEVICE_PTRS
+    a.stream = stream.cuda_stream if stream is not None else None
     keep = []
     if forced is not None:
         for key, field in (("forced_meas", "forced_meas"), ("fault_offsets", "fault_offsets"),
@@ -130,6 +133,40 @@ def test_noalloc_matches_sample_on_forced_replay():
     ref = _call("clifft_gpu_sample", prog, shots, 0, "fp64", flags, forced)
     first = _call("clifft_gpu_sample_noalloc", prog, shots, 0, "fp64", flags, forced)
     second = _call("clifft_gpu_sample_noalloc", prog, shots, 0, "fp64", flags, forced)
+    _same(first, ref)
+    _same(second, ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_noalloc_orders_its_work_on_the_callers_stream(precision):
+    # clear, launch and read-back of the static scratch all go on args->stream
+    torch = _torch()
+    from clifft_b200 import _native as N
+    prog = _program("cfg1")
+    shots, seed, flags = 20000, 91, N.CLIFFT_GPU_SURVIVORS
+    ref = _call("clifft_gpu_sample", prog, shots, seed, precision, flags)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        first = _call("clifft_gpu_sample_noalloc", prog, shots, seed, precision, flags, stream=s)
+        second = _call("clifft_gpu_sample_noalloc", prog, shots, seed, precision, flags, stream=s)
+    _same(first, ref)
+    _same(second, ref)
+
+
+def test_noalloc_on_a_second_device():
+    # the scratch address is looked up per device
+    torch = _torch()
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one CUDA device visible")
+    from clifft_b200 import _native as N
+    prog = _program("cfg1")
+    shots, seed, flags = 5000, 13, N.CLIFFT_GPU_SURVIVORS
+    try:
+        ref = _call("clifft_gpu_sample", prog, shots, seed, "fp32", flags, device=1)
+        first = _call("clifft_gpu_sample_noalloc", prog, shots, seed, "fp32", flags, device=1)
+        second = _call("clifft_gpu_sample_noalloc", prog, shots, seed, "fp32", flags, device=1)
+    finally:
+        torch.cuda.set_device(0)
     _same(first, ref)
     _same(second, ref)
 
