@@ -410,34 +410,58 @@ struct Tally {
 };
 
 // ------------------------------------------------------------- fused sweeps
-// A fused block is a run of consecutive array / frame opcodes whose active
-// axes fit in one tile of 2^TILE_BITS amplitudes. Its frame-dependent choices
-// (conjugated phases, U2 / U4 variants) are resolved once per shot into
-// micro-ops on tile-local bit positions; the statevector is then streamed tile
-// by tile through shared memory, applying every micro-op before writing back.
-// Each amplitude sees the same arithmetic in the same order as the unfused
-// opcode sequence.
-enum : uint8_t { M_CNOT, M_CZ, M_SWAP, M_MCNOT, M_MCZ, M_H, M_PHASE, M_U2, M_U4 };
-struct MicroOp {
-    uint8_t kind, a, b, pad;
-    uint32_t mask;  // local-bit mask (multi gates)
-    double c[32];   // up to 16 complex coefficients
+// A fused block is a run of consecutive opcodes applied to the statevector in
+// one streamed pass: tile by tile through shared memory, every micro-op of
+// the block on a tile before it is written back. A tile covers the tile axes
+// F (2^TILE_BITS amplitudes: every index with fixed values of the other,
+// tile-global axes). The block's frame-dependent choices (conjugated phases,
+// U2 / U4 variants, EXPAND phases) are resolved once per shot into micro-ops
+// on tile-local bit positions; each amplitude sees the same arithmetic in the
+// same order as the unfused opcode sequence.
+//   * Axes an op moves amplitudes along (targets of CNOT / SWAP / H / U2 / U4,
+//     the new axis of an EXPAND) must be tile axes. Control and parity axes
+//     may be tile-global: their bits are constant over a tile and enter the
+//     micro-op's condition through `greq` / `gpar`. Diagonal ops (CZ,
+//     multi-CZ, phases) therefore fuse whatever their axes.
+//   * EXPAND is a micro-op (copy the new axis' clear half onto its set half,
+//     times the phase); the block loads only the runs of each tile whose new
+//     axes are clear.
+//   * An active measurement on axis k-1 ends a block: its two half-norms are
+//     summed from the tile after the block's micro-ops (an X-basis
+//     measurement first folds with an H micro-op, a fused swap with a SWAP
+//     micro-op), and the collapse to the upper half flips the shot's address
+//     label (`xo`) instead of copying it.
+enum : uint8_t { M_CNOT, M_CZ, M_SWAP, M_MCNOT, M_MCZ, M_H, M_PHASE, M_U2, M_U4, M_EXPAND, M_SCALE };
+enum : uint8_t {
+    MF_PARITY = 0x1,  // the condition also needs odd parity of (index & par) ^ (global bits & gpar)
+    MF_COPY = 0x2,    // EXPAND without a phase: a plain copy
+};
+template <typename T>
+struct MicroOpT {
+    uint8_t kind, a, b, flags;  // a, b: tile-local target bits
+    uint32_t req;               // tile-local bits that must all be set
+    uint32_t par;               // tile-local parity bits (MF_PARITY)
+    uint32_t pad;
+    uint64_t greq;              // tile-global index bits that must all be set
+    uint64_t gpar;              // tile-global parity bits (MF_PARITY)
+    T c[16];                    // coefficients, already in the statevector's precision
 };
 constexpr int kMaxStages = 4;      // tile buffers (tiles in flight) per shot group: 2..4, chosen per launch
 constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 // Tile-engine geometry of a one-shot group. A CTA streams 32 KiB tiles and
 // fuses up to 24 opcodes per pass; a warp running one shot streams 4 KiB
-// tiles through two buffers and fuses up to 16, which leaves room for four
-// 4-warp CTAs per SM (the register limit). Scratch layout of one group: [kMaxStages
-// mbarriers][micro-ops][64 run offsets][64-byte axis -> local bit table]
-// [stages tile buffers, 128-B aligned].
+// tiles through two buffers and fuses up to 24 (FP32) / 16 (FP64), which
+// leaves room for four 4-warp CTAs per SM (the register limit). Scratch
+// layout of one group: [kMaxStages mbarriers][micro-ops][64 run offsets]
+// [64-byte axis -> local bit table][stages tile buffers, 128-B aligned].
 template <typename R, bool CTA>
 struct TileCfg {
+    using MOp = MicroOpT<typename Cx<R>::T>;
     static constexpr int kBits = CTA ? (sizeof(R) == 4 ? 12 : 11) : (sizeof(R) == 4 ? 9 : 8);
-    static constexpr int kMops = CTA ? 24 : 16;
+    static constexpr int kMops = CTA ? 24 : (sizeof(R) == 4 ? 24 : 16);
     static constexpr uint32_t kBarOffset = 0;
     static constexpr uint32_t kMopsOffset = kMaxStages * 8u;
-    static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MicroOp);
+    static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MOp);
     static constexpr uint32_t kLbitOffset = kTablesOffset + 64u * 8u;
     static constexpr uint32_t kBufOffset = (kLbitOffset + 64u + 127u) & ~127u;
     static __host__ __device__ constexpr uint32_t smem_bytes(uint32_t stages) {
@@ -548,12 +572,19 @@ struct Shot {
     bool solo;                 // CTA groups: only the control warp is executing
     int n_mops;
     unsigned long long moved;  // statevector bytes actually streamed
+    // Address label of a one-shot group's global statevector: logical
+    // amplitude i lives at v[i ^ xo]. A measurement that keeps the upper half
+    // of axis k-1 flips bit k-1 instead of copying that half down. Its bits
+    // are all above the tile bits, so the label maps every tile run to one
+    // contiguous run.
+    uint64_t xo;
+    uint64_t tileF;  // tile axes of the fused block being resolved
 
     __device__ __forceinline__ Shot(const DevProg& p, const KParams& kp, T* vv, uint32_t* r, uint32_t* d,
                                     uint32_t* o, double* rd, unsigned char* fz, uint32_t* bp, uint64_t s)
         : P(p), K(kp), v(vv), rec(r), det(d), obs(o), red(rd), shot(s), fuse(fz), bar_phase(bp) {}
 
-    __device__ __forceinline__ T& A(uint64_t i) { return v[i * S]; }
+    __device__ __forceinline__ T& A(uint64_t i) { return v[(kTiles ? (i ^ xo) : i) * S]; }
     // algorithmic bytes of an opcode (per-opcode definition); streamed bytes
     // are counted separately because a fused block streams the state once
     __device__ __forceinline__ void account(uint64_t amps) {
@@ -594,9 +625,16 @@ struct Shot {
         double g = hypot(gamma.x, gamma.y);
         if (g > hi || (g < lo && g > 0.0)) {
             uint64_t n = 1ull << k;
-            for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) A(i) = cscale(A(i), (R)g);
-            Grp::sync();
-            account(2 * n);
+            if (kTiles && resolving) {
+                // inside a fused block: the same scaling as a micro-op at this point
+                const double c[2] = {g, 0.0};
+                emit(M_SCALE, 0, 0, 0, 0, 0, c, 1);
+                bytes += 2 * n * sizeof(T);
+            } else {
+                for (uint64_t i = Grp::rank(); i < n; i += Grp::size()) A(i) = cscale(A(i), (R)g);
+                Grp::sync();
+                account(2 * n);
+            }
             gamma.x /= g;
             gamma.y /= g;
         }
@@ -725,6 +763,7 @@ struct Shot {
 
     // micro-op emission while resolving a fused block (thread 0 writes; every
     // thread computes the same values)
+    using MOp = typename TC::MOp;
     __device__ __forceinline__ uint8_t local_bit(uint32_t axis) const {
         return reinterpret_cast<const uint8_t*>(fuse + fuse_lbit_offset())[axis];
     }
@@ -732,20 +771,31 @@ struct Shot {
     static __host__ __device__ constexpr uint32_t fuse_mops_offset() { return TC::kMopsOffset; }
     static __host__ __device__ constexpr uint32_t fuse_tables_offset() { return TC::kTablesOffset; }
     static __host__ __device__ constexpr uint32_t fuse_lbit_offset() { return TC::kLbitOffset; }
-    __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t mask, const double* c,
-                                         int nc) {
-        MicroOp* m = reinterpret_cast<MicroOp*>(fuse + fuse_mops_offset()) + n_mops;
+    // local image of an axis mask (its bits on tile axes)
+    __device__ __forceinline__ uint32_t local_mask(uint64_t axes) const {
+        uint32_t lm = 0;
+        for (uint64_t w = axes & tileF; w; w &= w - 1) lm |= 1u << local_bit((uint32_t)__ffsll((long long)w) - 1);
+        return lm;
+    }
+    // a, b: target axes (tile axes); req / par: condition axes (any);
+    // coefficients c (nc complex values, converted to the statevector's
+    // precision as the unfused handlers convert them)
+    __device__ __forceinline__ void emit(uint8_t kind, uint32_t a, uint32_t b, uint64_t req, uint64_t par,
+                                         uint8_t flags, const double* c, int nc) {
+        MOp* m = reinterpret_cast<MOp*>(fuse + fuse_mops_offset()) + n_mops;
         if (Grp::rank() == 0) {
             m->kind = kind;
             m->a = local_bit(a);
             m->b = local_bit(b);
-            uint32_t lm = 0;
-            for (uint64_t w = mask; w; w &= w - 1) lm |= 1u << local_bit((uint32_t)__ffsll((long long)w) - 1);
-            m->mask = lm;
+            m->flags = flags;
+            m->req = local_mask(req);
+            m->par = local_mask(par);
+            m->greq = req & ~tileF;
+            m->gpar = par & ~tileF;
         }
-        // coefficients (up to 32 doubles of a U4 node) copied one per thread:
-        // one global-load latency instead of a serial chain of them
-        for (int j = Grp::rank(); j < nc; j += Grp::size()) m->c[j] = c[j];
+        // coefficients (up to 16 complex values of a U4 node) converted one
+        // per thread: one global-load latency instead of a serial chain
+        for (int j = Grp::rank(); j < nc; j += Grp::size()) m->c[j] = Cx<R>::make(c[2 * j], c[2 * j + 1]);
         n_mops++;
     }
 
@@ -753,7 +803,7 @@ struct Shot {
     __device__ __forceinline__ void array_cnot(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), cb = 1ull << c, tb = 1ull << t;
         if (kTiles && resolving) {
-            emit(M_CNOT, c, t, 0, nullptr, 0);
+            emit(M_CNOT, t, t, 1ull << c, 0, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, c, t) | cb; p.x = A(p.i); p.y = A(p.i | tb); return p; },
                       [&](const P2& p) { A(p.i) = p.y; A(p.i | tb) = p.x; });
@@ -766,7 +816,7 @@ struct Shot {
     __device__ __forceinline__ void array_cz(uint32_t c, uint32_t t) {
         const uint64_t n = 1ull << (k - 2), both = (1ull << c) | (1ull << t);
         if (kTiles && resolving) {
-            emit(M_CZ, c, t, 0, nullptr, 0);
+            emit(M_CZ, c, t, (1ull << c) | (1ull << t), 0, 0, nullptr, 0);
         } else {
             sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins00(i, c, t) | both; p.x = A(p.i); return p; },
                       [&](const P1& p) { A(p.i) = cneg(p.x); });
@@ -779,7 +829,7 @@ struct Shot {
     __device__ __forceinline__ void array_swap(uint32_t a, uint32_t b) {
         const uint64_t n = 1ull << (k - 2), ab = 1ull << a, bb = 1ull << b;
         if (kTiles && resolving) {
-            emit(M_SWAP, a, b, 0, nullptr, 0);
+            emit(M_SWAP, a, b, 0, 0, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins00(i, a, b); p.x = A(p.i | ab); p.y = A(p.i | bb); return p; },
                       [&](const P2& p) { A(p.i | ab) = p.y; A(p.i | bb) = p.x; });
@@ -792,7 +842,7 @@ struct Shot {
     __device__ __forceinline__ void array_multi_cnot(uint32_t t, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), tb = 1ull << t;
         if (kTiles && resolving) {
-            emit(M_MCNOT, t, t, mask, nullptr, 0);
+            emit(M_MCNOT, t, t, 0, mask & ~tb, MF_PARITY, nullptr, 0);
         } else {
             sweep<P2>(n,
                       [&](uint64_t i) {
@@ -822,7 +872,7 @@ struct Shot {
     __device__ __forceinline__ void array_multi_cz(uint32_t c, uint64_t mask) {
         const uint64_t n = 1ull << (k - 1), cb = 1ull << c;
         if (kTiles && resolving) {
-            emit(M_MCZ, c, c, mask, nullptr, 0);
+            emit(M_MCZ, c, c, cb, mask, MF_PARITY, nullptr, 0);
         } else {
             sweep<P1>(n,
                       [&](uint64_t i) {
@@ -848,7 +898,7 @@ struct Shot {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         const R s = (R)CGPU_INV_SQRT2;
         if (kTiles && resolving) {
-            emit(M_H, a, a, 0, nullptr, 0);
+            emit(M_H, a, a, 0, 0, 0, nullptr, 0);
         } else {
             sweep<P2>(n, [&](uint64_t i) { P2 p; p.i = ins0(i, a); p.x = A(p.i); p.y = A(p.i | ab); return p; },
                       [&](const P2& p) {
@@ -865,7 +915,7 @@ struct Shot {
         const uint64_t n = 1ull << (k - 1), ab = 1ull << a;
         if (kTiles && resolving) {
             const double c[2] = {re, im};
-            emit(M_PHASE, a, a, 0, c, 2);
+            emit(M_PHASE, a, a, ab, 0, 0, c, 1);
         } else {
             const T ph = Cx<R>::make(re, im);
             sweep<P1>(n, [&](uint64_t i) { P1 p; p.i = ins0(i, a) | ab; p.x = A(p.i); return p; },
@@ -910,13 +960,24 @@ struct Shot {
         const uint64_t half = 1ull << k;
         int x = with_phase ? f.px(a) : 0;
         const T ph = Cx<R>::make(with_phase ? zr : 1.0, with_phase ? (x ? -zi : zi) : 0.0);
+        if (kTiles && resolving) {
+            // inside a fused block: the new axis is a tile axis and the copy a micro-op
+            const double c[2] = {with_phase ? zr : 1.0, with_phase ? (x ? -zi : zi) : 0.0};
+            emit(M_EXPAND, a, a, 0, 0, with_phase ? 0 : MF_COPY, c, 1);
+            bytes += (2ull << k) * sizeof(T);
+            k++;
+            scale_magnitude(CGPU_EXPAND_SCALE);
+            if (with_phase && x) phase(make_double2(zr, zi));
+            return;
+        }
         if (tiled(k)) {
             if constexpr (kTiles) {
                 constexpr uint32_t MB = TC::kBits, TN = 1u << MB;
                 set_runs_low();
                 const int tid = Grp::rank(), nthr = Grp::size();
                 cur_site = 1;
-                stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, 0, half, 1, [&](T* buf, uint64_t) {
+                stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, 0, half, 1, 0,
+                             [&](T* buf, uint64_t, uint64_t) {
                     if (with_phase)
                         for (uint32_t l = tid; l < TN; l += nthr) buf[l] = cmul(buf[l], ph);
                     Grp::sync();
@@ -953,7 +1014,7 @@ struct Shot {
         Frame<NW>::put(f.z, a, (out >> 1) & 1);
         if (a >= k) return;
         if (kTiles && resolving) {
-            emit(M_U2, a, a, 0, m, 8);
+            emit(M_U2, a, a, 0, 0, 0, m, 4);
             account(2ull << k);
             return;
         }
@@ -980,7 +1041,7 @@ struct Shot {
         Frame<NW>::put(f.x, hi, (out >> 2) & 1);
         Frame<NW>::put(f.z, hi, (out >> 3) & 1);
         if (kTiles && resolving) {
-            emit(M_U4, lo, hi, 0, e, 32);
+            emit(M_U4, lo, hi, 0, 0, 0, e, 16);
             account(2ull << k);
             return;
         }
@@ -1089,7 +1150,6 @@ struct Shot {
     // (svm_forced_kernels.cc:112-158)
     __device__ __forceinline__ void meas_diagonal(uint32_t a, uint32_t idx, int sign) {
         const uint64_t half = 1ull << (k - 1);
-        int pxv = f.px(a), pzv = f.pz(a);
         double acc[2] = {0.0, 0.0};
         const bool tl = tiled(k);
         if (tl) {
@@ -1099,15 +1159,16 @@ struct Shot {
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint64_t ntiles = 1ull << (k - MB);
                 cur_site = 2;
-                stream_tiles(ntiles, ((1ull << k) - 1) & ~(uint64_t)(TN - 1), MB, 0, 0, 0, [&](T* buf, uint64_t t) {
-                    double q = 0.0;
-                    for (uint32_t l = tid; l < TN; l += nthr) q += cnorm_d(buf[l]);
-                    if (t >= ntiles / 2)
-                        acc[1] += q;
-                    else
-                        acc[0] += q;
-                    Grp::sync();
-                });
+                stream_tiles(ntiles, ((1ull << k) - 1) & ~(uint64_t)(TN - 1), MB, 0, 0, 0, 0,
+                             [&](T* buf, uint64_t t, uint64_t) {
+                                 double q = 0.0;
+                                 for (uint32_t l = tid; l < TN; l += nthr) q += cnorm_d(buf[l]);
+                                 if (t >= ntiles / 2)
+                                     acc[1] += q;
+                                 else
+                                     acc[0] += q;
+                                 Grp::sync();
+                             });
                 moved += (1ull << k) * sizeof(T);
             }
         } else {
@@ -1133,7 +1194,17 @@ struct Shot {
             bytes += (1ull << k) * sizeof(T);
         else
             account(1ull << k);
-        double p0 = acc[0], p1 = acc[1], total = p0 + p1;
+        diag_tail(a, idx, sign, acc[0], acc[1], false);
+    }
+    // Outcome, collapse and bookkeeping of a diagonal measurement of axis
+    // a = k-1 with half-norms p0 (bit a clear) and p1. relabel: the state
+    // was summed by a fused block and the b = 1 half becomes the state by
+    // flipping the address label; otherwise it is copied down (the
+    // reference's step, counted in the algorithmic bytes either way).
+    __device__ __forceinline__ void diag_tail(uint32_t a, uint32_t idx, int sign, double p0, double p1, bool relabel) {
+        const uint64_t half = 1ull << (k - 1);
+        const int pxv = f.px(a), pzv = f.pz(a);
+        const double total = p0 + p1;
         if (zero_norm(total)) return;
         int want = forced_bit(idx);
         if (want >= 0) want = want ^ sign ^ pxv;
@@ -1147,12 +1218,16 @@ struct Shot {
         int m_abs = b ^ pxv;
         if (b == 1 && pzv) negate_gamma();
         if (b == 1) {
-            if (tl) {
+            if (relabel) {
+                if constexpr (kTiles) xo ^= half;
+                bytes += (1ull << k) * sizeof(T);
+            } else if (tiled(k)) {
                 if constexpr (kTiles) {
                     constexpr uint32_t MB = TC::kBits, TN = 1u << MB;
+                    set_runs_low();
                     cur_site = 3;
-                    stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, half, 0, 1,
-                                 [&](T*, uint64_t) { Grp::sync(); });
+                    stream_tiles(half >> MB, (half - 1) & ~(uint64_t)(TN - 1), MB, half, 0, 1, 0,
+                                 [&](T*, uint64_t, uint64_t) { Grp::sync(); });
                     moved += (1ull << k) * sizeof(T);
                     bytes += (1ull << k) * sizeof(T);
                 }
@@ -1179,7 +1254,6 @@ struct Shot {
     __device__ __forceinline__ void meas_interfere(uint32_t fa, uint32_t t, uint32_t idx, int sign) {
         const bool swapped = fa != t;
         if (swapped) frame_swap(fa, t);
-        int pxv = f.px(t), pzv = f.pz(t);
         const uint64_t half = 1ull << t, fb = 1ull << fa;
         double acc[2] = {0.0, 0.0};
         // tiled path: the tile spans axes {fa, t} (t is its top local bit);
@@ -1197,7 +1271,7 @@ struct Shot {
                 const int tid = Grp::rank(), nthr = Grp::size();
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
                 cur_site = 4;
-                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, 0, [&](T* buf, uint64_t) {
+                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, 0, 0, [&](T* buf, uint64_t, uint64_t) {
                     double qp = 0.0, qm = 0.0;
                     for (uint32_t l = tid; l < HN; l += nthr) {
                         uint32_t a0 = swapped ? ((l & ~lfb) | (((l >> lf) & 1u) << lt)) : l;
@@ -1239,7 +1313,8 @@ struct Shot {
             bytes += ((1ull << k) * 2 + (1ull << (k - 1))) * sizeof(T);
         else
             account((1ull << k) * 2 + (1ull << (k - 1)));
-        double pp = acc[0], pm = acc[1], total = pp + pm;
+        const int pxv = f.px(t), pzv = f.pz(t);
+        const double pp = acc[0], pm = acc[1], total = pp + pm;
         if (zero_norm(total)) return;
         int want = forced_bit(idx);
         if (want >= 0) want = want ^ sign ^ pzv;
@@ -1250,7 +1325,6 @@ struct Shot {
             stop = true;
             return;
         }
-        int m_abs = bx ^ pzv;
         const R s = (R)CGPU_INV_SQRT2;
         if (tl) {
             if constexpr (kTiles) {
@@ -1259,7 +1333,7 @@ struct Shot {
                 const uint32_t lt = MB - 1, lfb = 1u << lf, HN = 1u << lt;
                 const uint32_t nruns = 1u << (MB - tr);
                 cur_site = 5;
-                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, nruns / 2, [&](T* buf, uint64_t) {
+                stream_tiles(1ull << (k - MB), tC, tr, 0, 0, nruns / 2, 0, [&](T* buf, uint64_t, uint64_t) {
                     if (!swapped) {
                         for (uint32_t l = tid; l < HN; l += nthr) {
                             T x = buf[l], y = buf[l + HN];
@@ -1301,7 +1375,14 @@ struct Shot {
                 Grp::sync();
             }
         }
-        double pb = bx ? pm : pp;
+        interfere_tail(swapped, t, idx, sign, pxv, pzv, bx, pp, pm, prob);
+    }
+    // Bookkeeping of an X-basis measurement of axis t = k-1 after its fold:
+    // branch bx with pp / pm the +/- branch weights.
+    __device__ __forceinline__ void interfere_tail(bool swapped, uint32_t t, uint32_t idx, int sign, int pxv, int pzv,
+                                                   int bx, double pp, double pm, double prob) {
+        const int m_abs = bx ^ pzv;
+        const double pb = bx ? pm : pp, total = pp + pm;
         if (!swapped) {
             if (pxv && m_abs) negate_gamma();
             k--;
@@ -1314,6 +1395,35 @@ struct Shot {
         Frame<NW>::put(f.x, t, m_abs);
         Frame<NW>::put(f.z, t, 0);
         write_meas(idx, m_abs ^ sign, prob);
+    }
+    // The measurement that ends a fused block: the block already applied the
+    // fold's arithmetic as micro-ops (SWAP f<->t if fused, then H on t, so the
+    // bit-t clear half holds (x + y) / sqrt2 and the set half (x - y) / sqrt2)
+    // and summed the two halves' norms (w0 bit t clear, w1 set; each 1/2 of
+    // the reference's |x +- y|^2 sums, which leaves every ratio unchanged).
+    // Branch bx keeps the half with bit t = bx: the address label flips for
+    // bx = 1. Diagonal measurements go to diag_tail.
+    __device__ __forceinline__ void interfere_relabel(uint32_t fa, uint32_t t, uint32_t idx, int sign, double w0,
+                                                      double w1) {
+        const bool swapped = fa != t;
+        if (swapped) frame_swap(fa, t);
+        bytes += ((1ull << k) * 2 + (1ull << (k - 1))) * sizeof(T);
+        const int pxv = f.px(t), pzv = f.pz(t);
+        const double total = w0 + w1;
+        if (zero_norm(total)) return;
+        int want = forced_bit(idx);
+        if (want >= 0) want = want ^ sign ^ pzv;
+        double prob;
+        const int bx = choose(w0, w1, total, want, &prob);
+        if (bx < 0) {
+            reachable = false;
+            stop = true;
+            return;
+        }
+        if (bx == 1) {
+            if constexpr (kTiles) xo ^= 1ull << t;
+        }
+        interfere_tail(swapped, t, idx, sign, pxv, pzv, bx, w0, w1, prob);
     }
 
     // ------------------------------------------------- classical / noise
@@ -1580,19 +1690,22 @@ struct Shot {
 
     // One streamed pass over 2^(k_pass) amplitudes in tiles of 2^TILE_BITS:
     // tile t covers the run offsets `runoff` (shared table, 2^(TILE_BITS - r)
-    // runs of 2^r amplitudes) shifted by pdep(t, C). Loads come from
-    // v[load_add + ...], optional stores (the first `store_runs` runs of each
-    // tile) go to v[store_add + ...]. Bulk copies (TMA) run K.stages - 1
-    // tiles ahead; `compute(buf, t)` is called by every thread of the group
-    // and must synchronise the group before it returns. Returns false after a
+    // runs of 2^r amplitudes) shifted by tbase = pdep(t, C). Loads come from
+    // logical amplitudes load_add + ..., optional stores (the first
+    // `store_runs` runs of each tile) go to store_add + ...; every logical
+    // index is mapped through the address label (i ^ xo). Runs whose index
+    // has a bit of `skip` set are not loaded (their contents are made by the
+    // compute step). Bulk copies (TMA) run K.stages - 1 tiles ahead;
+    // `compute(buf, t, tbase)` is called by every thread of the group and
+    // must synchronise the group before it returns. Returns false after a
     // barrier timeout.
     uint32_t cur_pc = 0;   // instruction being executed (diagnostics)
     uint32_t cur_site = 0; // which statevector pass is streaming (diagnostics)
     template <class Compute>
     __device__ bool stream_tiles(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add, uint64_t store_add,
-                                 uint32_t store_runs, Compute compute) {
+                                 uint32_t store_runs, uint32_t skip, Compute compute) {
         if constexpr (!Grp::kCta) {
-            return stream_tiles_warp(ntiles, C, r, load_add, store_add, store_runs, compute);
+            return stream_tiles_warp(ntiles, C, r, load_add, store_add, store_runs, skip, compute);
         }
         constexpr uint32_t MB = TC::kBits;
         constexpr uint32_t TN = 1u << MB;
@@ -1602,6 +1715,8 @@ struct Shot {
         const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
         const uint32_t nruns = 1u << (MB - r);
         const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
+        const uint32_t load_bytes = (nruns >> __popc(skip)) * run_bytes;
+        const uint64_t lx = xo;
         // the issuing warp: warp 0 of a CTA group, the shot's own warp otherwise
         const bool issuer = Grp::kCta ? (threadIdx.x >> 5) == 0 : true;
         const int lane = threadIdx.x & 31;
@@ -1623,11 +1738,13 @@ struct Shot {
         uint64_t issue_base = 0;  // pdep(next tile to load, C)
         uint32_t issue_st = 0;    // its stage
         auto issue_next = [&]() {
-            if (lane == 0) mbar_expect_tx(&bars[issue_st], TN * (uint32_t)sizeof(T));
+            if (lane == 0) mbar_expect_tx(&bars[issue_st], load_bytes);
             __syncwarp();
             const uint64_t base = load_add + issue_base;
             for (uint32_t j = lane; j < nruns; j += 32)
-                bulk_load(bufs + issue_st * TN + (j << r), v + base + runoff[j], run_bytes, &bars[issue_st]);
+                if (!(j & skip))
+                    bulk_load(bufs + issue_st * TN + (j << r), v + ((base + runoff[j]) ^ lx), run_bytes,
+                              &bars[issue_st]);
             issue_base = next_base(issue_base);
             issue_st = issue_st + 1 == nst ? 0 : issue_st + 1;
         };
@@ -1660,7 +1777,7 @@ struct Shot {
                 issue_next();  // tile t + nst - 1
             }
             T* buf = bufs + st * TN;
-            compute(buf, t);
+            compute(buf, t, tbase);
             if (store_runs) {
                 const uint64_t base = store_add + tbase;
                 if constexpr (Grp::kCta) {
@@ -1669,22 +1786,9 @@ struct Shot {
                     Grp::sync();
                     if (issuer) {
                         for (uint32_t j = lane; j < store_runs; j += 32)
-                            bulk_store(v + base + runoff[j], buf + (j << r), run_bytes);
+                            bulk_store(v + ((base + runoff[j]) ^ lx), buf + (j << r), run_bytes);
                         bulk_commit();
                     }
-                } else {
-                    // a warp writes its 4 KiB tile back with 16-byte stores
-                    // from every lane: a bulk store per tile costs its issuing
-                    // warp more (queueing behind the SM's other copies, then
-                    // a wait before the buffer is refilled) than it saves
-                    const uint32_t clog = r + (sizeof(T) == 8 ? 0u : 1u) - 1u;  // 16-B chunks per run, log2
-                    const uint32_t nchunks = store_runs << clog;
-                    for (uint32_t c = lane; c < nchunks; c += 32) {
-                        const uint32_t j = c >> clog, w = c & ((1u << clog) - 1u);
-                        const uint4 val = reinterpret_cast<const uint4*>(buf + (j << r))[w];
-                        reinterpret_cast<uint4*>(v + base + runoff[j])[w] = val;
-                    }
-                    __syncwarp();
                 }
             }
         }
@@ -1727,7 +1831,7 @@ struct Shot {
     // copy group always completes.
     template <class Compute>
     __device__ bool stream_tiles_warp(uint64_t ntiles, uint64_t C, uint32_t r, uint64_t load_add,
-                                      uint64_t store_add, uint32_t store_runs, Compute compute) {
+                                      uint64_t store_add, uint32_t store_runs, uint32_t skip, Compute compute) {
         constexpr uint32_t TN = 1u << TC::kBits;
         T* bufs = reinterpret_cast<T*>(fuse + TC::kBufOffset);
         const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
@@ -1736,12 +1840,15 @@ struct Shot {
         const uint32_t wmask = (1u << clog) - 1u;
         const uint32_t load_chunks = (1u << (TC::kBits - r)) << clog;
         const uint32_t store_chunks = store_runs << clog;
+        const uint64_t lx = xo;
         auto next_base = [C](uint64_t b) { return ((b | ~C) + 1) & C; };
         auto load_tile = [&](T* dst, uint64_t tb) {
             const uint64_t base = load_add + tb;
             for (uint32_t c = lane; c < load_chunks; c += 32) {
                 const uint32_t j = c >> clog, w = c & wmask;
-                cp_async16(reinterpret_cast<uint4*>(dst + (j << r)) + w, reinterpret_cast<const uint4*>(v + base + runoff[j]) + w);
+                if (j & skip) continue;
+                cp_async16(reinterpret_cast<uint4*>(dst + (j << r)) + w,
+                           reinterpret_cast<const uint4*>(v + ((base + runoff[j]) ^ lx)) + w);
             }
             cp_async_commit();
         };
@@ -1756,12 +1863,13 @@ struct Shot {
             __syncwarp();
             const uint64_t nb = next_base(tbase);
             if (t + 1 < ntiles) load_tile(bufs + ((t + 1) & 1u) * TN, nb);
-            compute(buf, t);
+            compute(buf, t, tbase);
             if (store_runs) {
                 const uint64_t base = store_add + tbase;
                 for (uint32_t c = lane; c < store_chunks; c += 32) {
                     const uint32_t j = c >> clog, w = c & wmask;
-                    reinterpret_cast<uint4*>(v + base + runoff[j])[w] = reinterpret_cast<const uint4*>(buf + (j << r))[w];
+                    reinterpret_cast<uint4*>(v + ((base + runoff[j]) ^ lx))[w] =
+                        reinterpret_cast<const uint4*>(buf + (j << r))[w];
                 }
                 __syncwarp();
             }
@@ -1770,19 +1878,31 @@ struct Shot {
         return true;
     }
 
-    // Fused tile sweep starting at `pc` (one-shot groups, statevector in
-    // global memory, k > tile bits), ending before `limit`. Returns the number
-    // of instructions consumed, 0 when the opcode at `pc` cannot start a block.
+    // Fused block starting at `pc` (one-shot groups, statevector in global
+    // memory, k > tile bits), ending before `limit`. With fusion (max_ops >
+    // 1) EXPANDs join the block and an active measurement ends it. Returns
+    // the number of instructions consumed, 0 when the opcode at `pc` does not
+    // start a block worth streaming.
     __device__ uint32_t fused_block(uint32_t pc, int max_ops, uint32_t limit) {
         constexpr uint32_t MB = TC::kBits;
-        uint64_t uni = 0;
-        int nsweep = 0;
+        const bool wide = max_ops > 1;
+        uint64_t need = 0;   // axes that must be tile axes
+        uint64_t fresh = 0;  // axes the block's EXPANDs create
+        int slots = 0;       // micro-op slots (an EXPAND reserves one for a renormalisation)
+        int nsweep = 0;      // array opcodes that touch the statevector
+        uint32_t kk = k;     // k after the instructions admitted so far
         uint32_t end = pc;
+        uint32_t term = 0;   // the terminating measurement's pc
+        int term_kind = 0;   // 1 diagonal, 2 X-basis, 3 X-basis with a fused swap
         for (; end < limit; ++end) {
             const uint4 w0 = __ldg(P.instr + 2 * end);
-            const uint32_t op = w0.x & 0xffu, x1 = w0.y & 0xffffu, x2 = w0.y >> 16;
-            uint64_t m = 0;
-            bool ok = true;
+            uint32_t op = w0.x & 0xffu;
+            const uint32_t x1 = w0.y & 0xffffu, x2 = w0.y >> 16;
+            if (op >= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED && op <= CLIFFT_OP_SWAP_MEAS_INTERFERE_FORCED)
+                op -= CLIFFT_OP_MEAS_DORMANT_STATIC_FORCED - CLIFFT_OP_MEAS_DORMANT_STATIC;
+            uint64_t nd = 0;
+            int cost = 0, tk = 0;
+            bool expand_op = false, ok = true;
             switch (op) {
                 case CLIFFT_OP_FRAME_CNOT:
                 case CLIFFT_OP_FRAME_CZ:
@@ -1790,76 +1910,175 @@ struct Shot {
                 case CLIFFT_OP_FRAME_S:
                 case CLIFFT_OP_FRAME_S_DAG:
                 case CLIFFT_OP_FRAME_SWAP: break;
-                case CLIFFT_OP_ARRAY_CNOT:
-                case CLIFFT_OP_ARRAY_CZ:
+                case CLIFFT_OP_ARRAY_CNOT: nd = 1ull << x2; cost = 1; break;          // the target moves
+                case CLIFFT_OP_ARRAY_MULTI_CNOT: nd = 1ull << x1; cost = 1; break;    // the target moves
                 case CLIFFT_OP_ARRAY_SWAP:
-                case CLIFFT_OP_ARRAY_U4: m = (1ull << x1) | (1ull << x2); break;
-                case CLIFFT_OP_ARRAY_MULTI_CNOT:
-                case CLIFFT_OP_ARRAY_MULTI_CZ: m = (((uint64_t)w0.w << 32) | w0.z) | (1ull << x1); break;
-                case CLIFFT_OP_ARRAY_H:
+                case CLIFFT_OP_ARRAY_U4: nd = (1ull << x1) | (1ull << x2); cost = 1; break;
+                case CLIFFT_OP_ARRAY_H: nd = 1ull << x1; cost = 1; break;
+                case CLIFFT_OP_ARRAY_CZ:
+                case CLIFFT_OP_ARRAY_MULTI_CZ:
                 case CLIFFT_OP_ARRAY_S:
-                case CLIFFT_OP_ARRAY_S_DAG: m = 1ull << x1; break;
+                case CLIFFT_OP_ARRAY_S_DAG: cost = 1; break;                           // diagonal: any axes
                 case CLIFFT_OP_ARRAY_T:
                 case CLIFFT_OP_ARRAY_T_DAG:
-                case CLIFFT_OP_ARRAY_ROT:
-                case CLIFFT_OP_ARRAY_U2: m = x1 < k ? (1ull << x1) : 0ull; break;
+                case CLIFFT_OP_ARRAY_ROT: cost = x1 < kk ? 1 : 0; break;
+                case CLIFFT_OP_ARRAY_U2:
+                    if (x1 < kk) {
+                        nd = 1ull << x1;
+                        cost = 1;
+                    }
+                    break;
+                case CLIFFT_OP_EXPAND:
+                case CLIFFT_OP_EXPAND_T:
+                case CLIFFT_OP_EXPAND_T_DAG:
+                case CLIFFT_OP_EXPAND_ROT:
+                    ok = wide;
+                    nd = 1ull << kk;
+                    cost = 2;
+                    expand_op = true;
+                    break;
+                case CLIFFT_OP_MEAS_ACTIVE_DIAGONAL: ok = wide; tk = 1; break;
+                case CLIFFT_OP_MEAS_ACTIVE_INTERFERE:
+                    ok = wide;
+                    tk = 2;
+                    nd = 1ull << (kk - 1);
+                    cost = 1;
+                    break;
+                case CLIFFT_OP_SWAP_MEAS_INTERFERE:
+                    ok = wide;
+                    tk = x1 != x2 ? 3 : 2;
+                    nd = (1ull << x1) | (1ull << x2);
+                    cost = tk == 3 ? 2 : 1;
+                    break;
                 default: ok = false;
             }
             if (!ok) break;
-            if (m) {
-                const uint64_t cand = uni | m;
+            const uint64_t cand = need | nd;
+            if ((uint32_t)__popcll(cand) > MB || slots + cost > max_ops) break;
+            if (nd) {
                 uint32_t rr;
-                if ((uint32_t)__popcll(cand) >= MB || nsweep >= max_ops) break;
                 tile_axes(cand, rr);
                 if (MB - rr > (uint32_t)kMaxRunsLog2) break;
-                uni = cand;
+            }
+            need = cand;
+            slots += cost;
+            if (expand_op) {
+                fresh |= 1ull << kk;
+                kk++;
+            } else if (cost && !tk) {
                 nsweep++;
             }
+            if (tk) {
+                term = end++;
+                term_kind = tk;
+                break;
+            }
         }
-        if (nsweep < 1) return 0;
+        // a block of EXPANDs alone costs more than the plain expansions
+        if (nsweep < 1 && !term_kind) return 0;
         uint32_t r;
-        const uint64_t F = tile_axes(uni, r);
-        const uint64_t C = ((k == 64) ? ~0ull : ((1ull << k) - 1)) & ~F;
+        const uint64_t F = tile_axes(need, r);
+        const uint64_t C = ((kk == 64) ? ~0ull : ((1ull << kk) - 1)) & ~F;
         uint8_t* lbit = reinterpret_cast<uint8_t*>(fuse + fuse_lbit_offset());
         if (Grp::rank() == 0) {
             uint32_t j = 0;
-            for (uint32_t a = 0; a < k; ++a)
-                if ((F >> a) & 1u) lbit[a] = (uint8_t)j++;
+            for (uint32_t a = 0; a < 64; ++a) lbit[a] = ((F >> a) & 1u) ? (uint8_t)j++ : (uint8_t)0xff;
         }
+        uint32_t skip = 0;  // run-index bits of the new axes: those runs are made, not loaded
+        for (uint64_t w = fresh; w; w &= w - 1) {
+            const uint32_t a = (uint32_t)__ffsll((long long)w) - 1;
+            skip |= 1u << ((uint32_t)__popcll(F & ((1ull << a) - 1)) - r);
+        }
+        tileF = F;
         set_runs(F, r);
         Grp::sync();
         // resolve the block's frame-dependent choices into micro-ops
         resolving = true;
         n_mops = 0;
-        for (uint32_t q = pc; q < end; ++q) exec(q);
+        const uint32_t rend = term_kind ? term : end;
+        for (uint32_t q = pc; q < rend; ++q) exec(q);
+        uint32_t tfa = 0, tt = 0, tidx = 0;
+        int tsign = 0;
+        bool red_local = false;
+        uint32_t red_bit = 0;
+        if (term_kind) {
+            const uint4 w0 = __ldg(P.instr + 2 * term);
+            cur_pc = term;
+            tfa = w0.y & 0xffffu;
+            tt = term_kind == 3 ? (w0.y >> 16) : tfa;
+            tidx = w0.z;
+            tsign = (((w0.x >> 16) & 0xffu) & CLIFFT_FLAG_SIGN) ? 1 : 0;
+            if (term_kind == 3) emit(M_SWAP, tfa, tt, 0, 0, 0, nullptr, 0);
+            if (term_kind >= 2) emit(M_H, tt, tt, 0, 0, 0, nullptr, 0);
+            red_local = ((F >> tt) & 1u) != 0;
+            red_bit = red_local ? (uint32_t)__popcll(F & ((1ull << tt) - 1)) : tt;
+        }
         resolving = false;
+        if (Grp::rank() == 0)
+            compile_index_runs(reinterpret_cast<MOp*>(fuse + fuse_mops_offset()), n_mops,
+                               (1u << MB) / (uint32_t)Grp::size());
         Grp::sync();
-        const MicroOp* mops = reinterpret_cast<const MicroOp*>(fuse + fuse_mops_offset());
+        const MOp* mops = reinterpret_cast<const MOp*>(fuse + fuse_mops_offset());
         const int tid = Grp::rank(), nthr = Grp::size();
         const int nm = n_mops;
         cur_site = 6;
         constexpr uint32_t TN = 1u << MB;
         const uint32_t rpt = TN / (uint32_t)nthr;  // amplitudes per thread in a register-staged run
-        stream_tiles(1ull << (k - MB), C, r, 0, 0, 1u << (MB - r), [&](T* buf, uint64_t) {
+        double acc[2] = {0.0, 0.0};
+        const uint32_t nruns = 1u << (MB - r);
+        stream_tiles(1ull << (kk - MB), C, r, 0, 0, nm ? nruns : 0, skip, [&](T* buf, uint64_t, uint64_t tbase) {
             for (int j = 0; j < nm;) {
                 int e = j;
                 while (e < nm && index_map_kind(mops[e].kind)) ++e;
                 if (e - j >= 2 && rpt <= kMaxRunAmps) {
                     if (kMaxRunAmps >= 16 && rpt == 16)
-                        apply_index_run<(kMaxRunAmps >= 16 ? 16 : 8)>(mops, j, e, buf, tid, nthr);
+                        apply_index_run<(kMaxRunAmps >= 16 ? 16 : 8)>(mops, j, e, buf, tid, nthr, tbase);
                     else if (rpt == 8)
-                        apply_index_run<8>(mops, j, e, buf, tid, nthr);
+                        apply_index_run<8>(mops, j, e, buf, tid, nthr, tbase);
                     else
-                        apply_index_run<4>(mops, j, e, buf, tid, nthr);
+                        apply_index_run<4>(mops, j, e, buf, tid, nthr, tbase);
                     j = e;
                     continue;
                 }
-                apply_micro(mops[j], buf, tid, nthr);
+                apply_micro(mops[j], buf, tid, nthr, tbase);
                 Grp::sync();
                 ++j;
             }
+            if (term_kind) {
+                // the measured axis' two half-norms of this tile
+                double q0 = 0.0, q1 = 0.0;
+                if (red_local) {
+                    for (uint32_t l = tid; l < TN; l += nthr) {
+                        const double q = cnorm_d(buf[l]);
+                        if ((l >> red_bit) & 1u)
+                            q1 += q;
+                        else
+                            q0 += q;
+                    }
+                } else {
+                    for (uint32_t l = tid; l < TN; l += nthr) q0 += cnorm_d(buf[l]);
+                    if ((tbase >> red_bit) & 1u) {
+                        q1 = q0;
+                        q0 = 0.0;
+                    }
+                }
+                acc[0] += q0;
+                acc[1] += q1;
+            }
+            Grp::sync();
         });
-        moved += (2ull << k) * sizeof(T);
+        moved += (((1ull << kk) >> __popcll(fresh)) + (nm ? (1ull << kk) : 0ull)) * sizeof(T);
+        if (term_kind) {
+            group_reduce<Grp, 2>(acc, red);
+            if (!stop) {
+                if (term_kind == 1) {
+                    bytes += (1ull << k) * sizeof(T);
+                    diag_tail(tt, tidx, tsign, acc[0], acc[1], true);
+                } else {
+                    interfere_relabel(tfa, tt, tidx, tsign, acc[0], acc[1]);
+                }
+            }
+        }
         return end - pc;
     }
 
@@ -1870,109 +2089,207 @@ struct Shot {
         return kind == M_CNOT || kind == M_SWAP || kind == M_MCNOT || kind == M_CZ || kind == M_MCZ ||
                kind == M_PHASE;
     }
+    // Condition of a conditional micro-op at tile position p, given its
+    // tile-global parity gp: every `req` bit set and, with MF_PARITY, odd
+    // parity of the `par` bits and gp.
+    static __device__ __forceinline__ bool micro_on(const MOp& m, uint32_t p, uint32_t gp) {
+        return (p & m.req) == m.req && (!(m.flags & MF_PARITY) || ((__popc(p & m.par) ^ gp) & 1u));
+    }
     static constexpr uint32_t kMaxRunAmps = sizeof(R) == 4 ? 16u : 8u;  // register budget of a staged run
-    // A run mops[j0, j1) of index-map micro-ops in one pass over the tile: each
-    // thread reads RPT amplitudes into registers, follows every amplitude's
-    // position through the run, applying the diagonal factors in the run's
-    // order (the same operations, in the same order, as one micro-op at a
-    // time), then writes each amplitude at its final position. The barrier
-    // between the read and write phases makes the in-place permutation safe.
-    template <int RPT>
-    static __device__ void apply_index_run(const MicroOp* mops, int j0, int j1, T* tile, int tid, int nthr) {
-        T v[RPT];
-        uint32_t pos[RPT];
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-            pos[q] = (uint32_t)(tid + q * nthr);
-            v[q] = tile[pos[q]];
+    // A run of index-map micro-ops is compiled once per block into an affine
+    // map over GF(2) of tile positions: after the run's first j ops an
+    // amplitude that started at position p0 sits at P_j = L_j p0 ^ b_j, where
+    // the linear part L_j depends only on the ops' tile-local bits and the
+    // offset b_j also on the tile's global bits (global controls, the global
+    // part of a multi gate's parity). CNOT / multi-CNOT / SWAP only update
+    // (L, b); a diagonal op's condition is an AND of affine bits of P_j, each
+    // the parity of p0 & row (the rows of L_j it reads) ^ a per-tile constant.
+    // The rows of each diagonal op and the final map's columns are kept in
+    // coefficient slots those ops do not use.
+    struct RunRows {
+        uint16_t row[3];
+        uint8_t n, pad;
+    };
+    static __device__ __forceinline__ RunRows* run_rows(MOp& m) { return reinterpret_cast<RunRows*>(&m.c[1]); }
+    static __device__ __forceinline__ const RunRows* run_rows(const MOp& m) {
+        return reinterpret_cast<const RunRows*>(&m.c[1]);
+    }
+    static __device__ __forceinline__ uint16_t* run_cols(MOp& m) { return reinterpret_cast<uint16_t*>(&m.c[4]); }
+    static __device__ __forceinline__ const uint16_t* run_cols(const MOp& m) {
+        return reinterpret_cast<const uint16_t*>(&m.c[4]);
+    }
+    // Compiles every run the tile loop will stage (the same boundaries: at
+    // least two consecutive index-map ops and rpt <= kMaxRunAmps). Run by one
+    // thread.
+    static __device__ void compile_index_runs(MOp* mops, int nm, uint32_t rpt) {
+        constexpr uint32_t MB = TC::kBits;
+        for (int j = 0; j < nm;) {
+            int e = j;
+            while (e < nm && index_map_kind(mops[e].kind)) ++e;
+            if (!(e - j >= 2 && rpt <= kMaxRunAmps)) {
+                ++j;
+                continue;
+            }
+            uint16_t rows[MB];  // P bit i = parity(p0 & rows[i]) ^ b bit i
+            for (uint32_t i = 0; i < MB; ++i) rows[i] = (uint16_t)(1u << i);
+            for (int q = j; q < e; ++q) {
+                MOp& m = mops[q];
+                auto par_row = [&](uint32_t par) {
+                    uint16_t x = 0;
+                    for (uint32_t w = par; w; w &= w - 1) x ^= rows[__ffs(w) - 1];
+                    return x;
+                };
+                switch (m.kind) {
+                    case M_CNOT:
+                        if (m.req) rows[m.a] ^= rows[__ffs(m.req) - 1];
+                        break;
+                    case M_MCNOT: rows[m.a] ^= par_row(m.par); break;
+                    case M_SWAP: {
+                        const uint16_t t = rows[m.a];
+                        rows[m.a] = rows[m.b];
+                        rows[m.b] = t;
+                        break;
+                    }
+                    default: {  // M_CZ, M_MCZ, M_PHASE
+                        RunRows* rr = run_rows(m);
+                        int n = 0;
+                        for (uint32_t w = m.req; w; w &= w - 1) rr->row[n++] = rows[__ffs(w) - 1];
+                        if (m.flags & MF_PARITY) rr->row[n++] = par_row(m.par);
+                        rr->n = (uint8_t)n;
+                        break;
+                    }
+                }
+            }
+            uint16_t* fc = run_cols(mops[j]);
+            for (uint32_t c = 0; c < MB; ++c) {
+                uint32_t col = 0;
+                for (uint32_t i = 0; i < MB; ++i) col |= ((rows[i] >> c) & 1u) << i;
+                fc[c] = (uint16_t)col;
+            }
+            j = e;
         }
+    }
+    // A compiled run mops[j0, j1) in one pass over the tile: each thread
+    // reads RPT amplitudes (positions tid + q * nthr) into registers, follows
+    // the run's affine offset through its ops (scalar work per tile), applies
+    // every diagonal factor in the run's order to the amplitudes it hits (the
+    // same operations, in the same order, as one micro-op at a time), then
+    // writes each amplitude at its final position. The barrier between the
+    // read and write phases makes the in-place permutation safe.
+    template <int RPT>
+    static __device__ void apply_index_run(const MOp* mops, int j0, int j1, T* tile, int tid, int nthr,
+                                           uint64_t tbase) {
+        constexpr uint32_t MB = TC::kBits;
+        constexpr uint32_t QB = RPT == 16 ? 4u : (RPT == 8 ? 3u : 2u);  // bits of the register index q
+        constexpr uint32_t ALL = (1u << RPT) - 1u;
+        const uint32_t lg = MB - QB;  // p0 = tid | q << lg
+        T v[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) v[q] = tile[tid + q * nthr];
+        // mask over q of parity(p0 & row) ^ k
+        auto bits = [&](uint32_t row, uint32_t k) -> uint32_t {
+            const uint32_t r = row >> lg;
+            uint32_t m = ((r & 1u) ? (0xAAAAu & ALL) : 0u) ^ ((r & 2u) ? (0xCCCCu & ALL) : 0u);
+            if (QB > 2) m ^= (r & 4u) ? (0xF0F0u & ALL) : 0u;
+            if (QB > 3) m ^= (r & 8u) ? (0xFF00u & ALL) : 0u;
+            const uint32_t t = ((uint32_t)__popc((uint32_t)tid & row & ((1u << lg) - 1u)) ^ k) & 1u;
+            return m ^ (0u - t) & ALL;
+        };
+        uint32_t b = 0;  // the run's affine offset so far
         for (int j = j0; j < j1; ++j) {
-            const MicroOp& m = mops[j];
-            const uint32_t ab = 1u << m.a, bb = 1u << m.b;
-            switch (m.kind) {
-                case M_CNOT:
+            const MOp& m = mops[j];
+            const uint64_t greq = m.greq;
+            if ((tbase & greq) != greq) continue;  // the op is the identity on this tile
+            const uint32_t kind = m.kind;
+            if (kind == M_CNOT) {
+                const uint32_t req = m.req;
+                b ^= (req ? ((b >> (__ffs(req) - 1)) & 1u) : 1u) << m.a;
+            } else if (kind == M_MCNOT) {
+                b ^= (((uint32_t)__popc(b & m.par) ^ (uint32_t)__popcll(tbase & m.gpar)) & 1u) << m.a;
+            } else if (kind == M_SWAP) {
+                const uint32_t d = ((b >> m.a) ^ (b >> m.b)) & 1u;
+                b ^= (0u - d) & ((1u << m.a) | (1u << m.b));
+            } else {
+                const RunRows rr = *run_rows(m);
+                uint32_t hit = ALL;
+                int n = 0;
+                for (uint32_t w = m.req; w; w &= w - 1) hit &= bits(rr.row[n++], (b >> (__ffs(w) - 1)) & 1u);
+                if (m.flags & MF_PARITY)
+                    hit &= bits(rr.row[n], ((uint32_t)__popc(b & m.par) ^ (uint32_t)__popcll(tbase & m.gpar)) & 1u);
+                if (kind == M_PHASE) {
+                    const T ph = m.c[0];
 #pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if (pos[q] & ab) pos[q] ^= bb;
-                    break;
-                case M_SWAP:
+                    for (int q = 0; q < RPT; ++q) {
+                        const T w = cmul(v[q], ph);
+                        v[q] = ((hit >> q) & 1u) ? w : v[q];
+                    }
+                } else {
 #pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if (((pos[q] >> m.a) ^ (pos[q] >> m.b)) & 1u) pos[q] ^= ab | bb;
-                    break;
-                case M_MCNOT:
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if (__popc(pos[q] & m.mask & ~ab) & 1) pos[q] ^= ab;
-                    break;
-                case M_CZ:
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if ((pos[q] & ab) && (pos[q] & bb)) v[q] = cneg(v[q]);
-                    break;
-                case M_MCZ:
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if ((pos[q] & ab) && (__popc(pos[q] & m.mask) & 1)) v[q] = cneg(v[q]);
-                    break;
-                default: {  // M_PHASE
-                    const T ph = Cx<R>::make(m.c[0], m.c[1]);
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-                        if (pos[q] & ab) v[q] = cmul(v[q], ph);
-                    break;
+                    for (int q = 0; q < RPT; ++q) v[q] = ((hit >> q) & 1u) ? cneg(v[q]) : v[q];
                 }
             }
         }
+        // final positions: L p0 ^ b, L applied column by column
+        const uint16_t* fc = run_cols(mops[j0]);
+        uint32_t lt = b;
+        for (uint32_t i = 0; i < lg; ++i) lt ^= ((tid >> i) & 1u) ? (uint32_t)fc[i] : 0u;
+        uint32_t cq[QB];
+#pragma unroll
+        for (uint32_t i = 0; i < QB; ++i) cq[i] = fc[lg + i];
         Grp::sync();
 #pragma unroll
-        for (int q = 0; q < RPT; ++q) tile[pos[q]] = v[q];
+        for (int q = 0; q < RPT; ++q) {
+            uint32_t pq = lt;
+#pragma unroll
+            for (uint32_t i = 0; i < QB; ++i)
+                if ((q >> i) & 1) pq ^= cq[i];
+            tile[pq] = v[q];
+        }
         Grp::sync();
     }
 
-    // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes; the
-    // arithmetic matches the unfused opcode handlers exactly.
-    static __device__ __forceinline__ void apply_micro(const MicroOp& m, T* tile, int tid, int nthr) {
+    // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes whose
+    // tile-global index bits are tbase; the arithmetic matches the unfused
+    // opcode handlers exactly.
+    static __device__ __forceinline__ void apply_micro(const MOp& m, T* tile, int tid, int nthr, uint64_t tbase) {
         constexpr uint32_t MB = TC::kBits;
+        if ((tbase & m.greq) != m.greq) return;  // the op is the identity on this tile
+        const uint32_t gp = (uint32_t)__popcll(tbase & m.gpar) & 1u;
         const uint32_t a = m.a, b = m.b;
         const uint32_t ab = 1u << a, bb = 1u << b;
         switch (m.kind) {
             case M_CNOT:
-                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t b0 = ins00_32(i, a, b) | ab;
-                    T x = tile[b0];
-                    tile[b0] = tile[b0 | bb];
-                    tile[b0 | bb] = x;
-                }
-                break;
-            case M_CZ:
-                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t idx = ins00_32(i, a, b) | ab | bb;
-                    tile[idx] = cneg(tile[idx]);
-                }
-                break;
-            case M_SWAP:
-                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
-                    uint32_t base = ins00_32(i, a, b);
-                    T x = tile[base | ab];
-                    tile[base | ab] = tile[base | bb];
-                    tile[base | bb] = x;
-                }
-                break;
             case M_MCNOT:
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = ins0_32(i, a);
-                    if (__popc(i0 & m.mask) & 1) {
+                    const uint32_t i0 = ins0_32(i, a);
+                    if (micro_on(m, i0, gp)) {
                         T x = tile[i0];
                         tile[i0] = tile[i0 | ab];
                         tile[i0 | ab] = x;
                     }
                 }
                 break;
+            case M_CZ:
             case M_MCZ:
-                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t i0 = ins0_32(i, a) | ab;
-                    if (__popc(i0 & m.mask) & 1) tile[i0] = cneg(tile[i0]);
+            case M_PHASE: {
+                // positions with every `req` bit set (at most two bits)
+                const uint32_t nreq = (uint32_t)__popc(m.req);
+                const uint32_t r0 = m.req ? (uint32_t)__ffs(m.req) - 1 : 0u;
+                const uint32_t r1 = nreq > 1 ? (uint32_t)__ffs(m.req & (m.req - 1)) - 1 : 0u;
+                const T ph = m.c[0];
+                for (uint32_t i = tid; i < (1u << (MB - nreq)); i += nthr) {
+                    const uint32_t idx = (nreq == 0 ? i : (nreq == 1 ? ins0_32(i, r0) : ins00_32(i, r0, r1))) | m.req;
+                    if (!micro_on(m, idx, gp)) continue;
+                    tile[idx] = m.kind == M_PHASE ? cmul(tile[idx], ph) : cneg(tile[idx]);
+                }
+                break;
+            }
+            case M_SWAP:
+                for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
+                    uint32_t base = ins00_32(i, a, b);
+                    T x = tile[base | ab];
+                    tile[base | ab] = tile[base | bb];
+                    tile[base | bb] = x;
                 }
                 break;
             case M_H: {
@@ -1985,17 +2302,8 @@ struct Shot {
                 }
                 break;
             }
-            case M_PHASE: {
-                const T ph = Cx<R>::make(m.c[0], m.c[1]);
-                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
-                    uint32_t idx = ins0_32(i, a) | ab;
-                    tile[idx] = cmul(tile[idx], ph);
-                }
-                break;
-            }
             case M_U2: {
-                const T m00 = Cx<R>::make(m.c[0], m.c[1]), m01 = Cx<R>::make(m.c[2], m.c[3]);
-                const T m10 = Cx<R>::make(m.c[4], m.c[5]), m11 = Cx<R>::make(m.c[6], m.c[7]);
+                const T m00 = m.c[0], m01 = m.c[1], m10 = m.c[2], m11 = m.c[3];
                 for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
                     uint32_t i0 = ins0_32(i, a);
                     T x = tile[i0], y = tile[i0 | ab];
@@ -2005,19 +2313,19 @@ struct Shot {
                 break;
             }
             case M_U4: {
-                // FP32: the 16 coefficients converted once and held in registers;
-                // FP64 reads them from shared memory (its registers are spoken for)
+                // FP32: the 16 coefficients held in registers; FP64 reads them
+                // from shared memory (its registers are spoken for)
                 constexpr bool kHoist = sizeof(R) == 4;
                 T cm[kHoist ? 16 : 1];
                 if constexpr (kHoist) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) cm[j] = Cx<R>::make(m.c[2 * j], m.c[2 * j + 1]);
+                    for (int j = 0; j < 16; ++j) cm[j] = m.c[j];
                 }
                 auto coef = [&](int j) -> T {
                     if constexpr (kHoist)
                         return cm[j];
                     else
-                        return Cx<R>::make(m.c[2 * j], m.c[2 * j + 1]);
+                        return m.c[j];
                 };
                 for (uint32_t i = tid; i < (1u << (MB - 2)); i += nthr) {
                     uint32_t q = ins00_32(i, a, b);
@@ -2036,6 +2344,21 @@ struct Shot {
                     tile[q | bb] = y[2];
                     tile[q | ab | bb] = y[3];
                 }
+                break;
+            }
+            case M_EXPAND: {
+                // the new axis' set half from its clear half (x the phase)
+                const T ph = m.c[0];
+                const bool copy = (m.flags & MF_COPY) != 0;
+                for (uint32_t i = tid; i < (1u << (MB - 1)); i += nthr) {
+                    const uint32_t i0 = ins0_32(i, a);
+                    tile[i0 | ab] = copy ? tile[i0] : cmul(tile[i0], ph);
+                }
+                break;
+            }
+            case M_SCALE: {
+                const R g = m.c[0].x;
+                for (uint32_t i = tid; i < (1u << MB); i += nthr) tile[i] = cscale(tile[i], g);
                 break;
             }
             default: break;
@@ -2271,6 +2594,8 @@ struct Shot {
         }
     }
     __device__ __forceinline__ void load_state() {
+        xo = 0;  // amplitudes come back in logical order
+        tileF = 0;
         const unsigned char* d = K.seg_state + shot * K.seg_stride;
         const uint64_t* w = reinterpret_cast<const uint64_t*>(d);
 #pragma unroll
@@ -2314,6 +2639,8 @@ struct Shot {
     __device__ __forceinline__ void reset() {
         // SchrodingerState::reset (svm_state.cc:220-267): only v[0] needs a
         // value; every other amplitude is written by EXPAND before it is read.
+        xo = 0;
+        tileF = 0;
         f.clear();
         gamma = make_double2(1.0, 0.0);
         k = 0;
