@@ -502,6 +502,7 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src_smem, uint
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
@@ -1767,12 +1768,11 @@ struct Shot {
                 break;
             }
             phase ^= 1u << st;
-            // refill the stage that held tile t-1 before computing tile t:
-            // every thread finished tile t-1 (compute ends with a group
-            // barrier) and its store has read the buffer once the bulk group
-            // drains, so nst-1 tiles stay in flight during the compute
-            if (issuer && t + nst - 1 < ntiles) {
-                if (Grp::kCta && store_runs) bulk_wait_read0();
+            // A pass without stores refills the stage that held tile t-1
+            // before computing tile t (every thread finished tile t-1: compute
+            // ends with a group barrier), so nst-1 tiles stay in flight during
+            // the compute. With stores see below.
+            if (issuer && !store_runs && t + nst - 1 < ntiles) {
                 __syncwarp();
                 issue_next();  // tile t + nst - 1
             }
@@ -1788,6 +1788,16 @@ struct Shot {
                         for (uint32_t j = lane; j < store_runs; j += 32)
                             bulk_store(v + ((base + runoff[j]) ^ lx), buf + (j << r), run_bytes);
                         bulk_commit();
+                        // Refill the stage of tile t-1 once its store (one bulk
+                        // group older than tile t's) has read the buffer: by now
+                        // a whole compute has passed since it was issued. Waiting
+                        // for it before the compute stalled the issuing warp for
+                        // most of a store, and the CTA with it at its next barrier.
+                        if (t + nst - 1 < ntiles) {
+                            bulk_wait_read1();
+                            __syncwarp();
+                            issue_next();  // tile t + nst - 1
+                        }
                     }
                 }
             }
@@ -2026,10 +2036,13 @@ struct Shot {
         const uint32_t rpt = TN / (uint32_t)nthr;  // amplitudes per thread in a register-staged run
         double acc[2] = {0.0, 0.0};
         const uint32_t nruns = 1u << (MB - r);
+        // an X-basis terminator's H is the block's last micro-op: applied
+        // together with the half-norm sums
+        const int nmo = term_kind >= 2 ? nm - 1 : nm;
         stream_tiles(1ull << (kk - MB), C, r, 0, 0, nm ? nruns : 0, skip, [&](T* buf, uint64_t, uint64_t tbase) {
-            for (int j = 0; j < nm;) {
+            for (int j = 0; j < nmo;) {
                 int e = j;
-                while (e < nm && index_map_kind(mops[e].kind)) ++e;
+                while (e < nmo && index_map_kind(mops[e].kind)) ++e;
                 if (e - j >= 2 && rpt <= kMaxRunAmps) {
                     if (kMaxRunAmps >= 16 && rpt == 16)
                         apply_index_run<(kMaxRunAmps >= 16 ? 16 : 8)>(mops, j, e, buf, tid, nthr, tbase);
@@ -2044,7 +2057,23 @@ struct Shot {
                 Grp::sync();
                 ++j;
             }
-            if (term_kind) {
+            if (term_kind >= 2) {
+                // H on the measured axis, summing the norms of both outputs
+                const uint32_t a = red_bit, ab = 1u << a;
+                const R s = (R)CGPU_INV_SQRT2;
+                double q0 = 0.0, q1 = 0.0;
+                for (uint32_t i = tid; i < (TN >> 1); i += nthr) {
+                    const uint32_t i0 = ins0_32(i, a);
+                    const T x = buf[i0], y = buf[i0 | ab];
+                    const T u = cscale(cadd(x, y), s), w = cscale(csub(x, y), s);
+                    buf[i0] = u;
+                    buf[i0 | ab] = w;
+                    q0 += cnorm_d(u);
+                    q1 += cnorm_d(w);
+                }
+                acc[0] += q0;
+                acc[1] += q1;
+            } else if (term_kind) {
                 // the measured axis' two half-norms of this tile
                 double q0 = 0.0, q1 = 0.0;
                 if (red_local) {
