@@ -17,8 +17,10 @@ time). `e2e` = the same metric through the public Python API
 (`clifft_b200.sample` on a freshly uploaded program, records read back and
 unpacked on the host). `extras` put the plain FP64 executor (one pass per
 opcode, fixed launch heuristic) beside it on the same workload, the k = 10 and
-k = 16 programs, the noisy memory-grid survivor workload, and the largest
-FP32-vs-FP64 measurement-probability difference.
+k = 16 programs, the noisy memory-grid survivor workload, the k = 24 program at
+10^3 shots with 128 resident, and (a check, not a timing) the largest FP32 and
+FP64 errors against the reference executor of every measurement probability
+and of the amplitudes at peak rank.
 
 `--impl reference` times the reference's own executor (oracle/_ref, built
 from the reference sources) on this host's cores on the same workload.
@@ -115,7 +117,8 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ GPU helpers
-def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False, group=0):
+def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False, group=0,
+               max_resident=0):
     """One device-resident sampling step: program resident, outputs in HBM.
     plain = the plain executor: one pass per opcode, fixed heuristic launch
     shape, one launch per call (no fusion, no autotuning, no survivor
@@ -129,7 +132,7 @@ def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=F
         flags |= N.CLIFFT_GPU_NO_FUSION | N.CLIFFT_GPU_NO_AUTOTUNE | N.CLIFFT_GPU_NO_SEGMENTS
     a = N.SampleArgs(shots=shots, seed=seed, first_shot=first_shot,
                      precision=N.CLIFFT_GPU_FP32 if precision == "fp32" else N.CLIFFT_GPU_FP64,
-                     flags=flags, group_threads=group, stream=stream.cuda_stream)
+                     flags=flags, group_threads=group, stream=stream.cuda_stream, max_resident=max_resident)
     o = N.Outputs()
     for field, t in bufs.items():
         setattr(o, field, t.data_ptr() if t.numel() else None)
@@ -151,7 +154,7 @@ def output_buffers(torch, prog, shots, dev):
 
 
 def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survivors=False, plain=False,
-                group=0):
+                group=0, max_resident=0):
     import clifft_b200 as cb
     dev = torch.device("cuda", torch.cuda.current_device())
     dp = cb.load(prog)
@@ -159,14 +162,14 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survi
     bufs = output_buffers(torch, prog, shots, dev)
     first = rank * shots
     for w in range(warmup):
-        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain, group)
+        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain, group, max_resident)
     torch.cuda.synchronize()
     times, kernel_ms, launches, passed, alg_bytes, streamed, groups = [], [], 0, 0, 0, 0, set()
     for s in range(steps):
         flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain, group)
+        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain, group, max_resident)
         ev1.record(stream)
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1))
@@ -204,21 +207,58 @@ def time_e2e(name, shots, steps, torch, first_shot=0):
     return times, h2d, d2h
 
 
-def prob_error(name, shots=8):
-    """Largest |p_FP32 - p_FP64| over every measurement of `shots` forced
-    trajectories (outcomes from an FP64 run of the same program)."""
+def reference_errors(name, shots):
+    """Largest error against the reference executor (oracle/_ref, FP64) of
+    every measurement probability of `shots` forced trajectories (outcomes of
+    an FP64 GPU run), and, for a prefix of the program that ends where k
+    first reaches its peak, of the normalised amplitudes (max abs, relative
+    L2, 1 - |overlap|), for the FP32 and FP64 statevectors. A check, not a
+    timing: the reference replays the same bytecode on the host."""
     import numpy as np
     import clifft_b200 as cb
+    from clifft_b200.program import ACTIVE_MEAS, Program
+    from oracle import pyoracle as O
+    if not O.ref_available():
+        return None
     prog = load_program(name)
-    f = cb.run(prog, shots, 5, precision="fp64", trace=True)
-    words = f["meas_words"]
-    bits = np.unpackbits(words.view(np.uint8), axis=1, bitorder="little")[:, :prog.num_measurements]
+    f = cb.run(prog, shots, 5, precision="fp64")
+    bits = cb.api._unpack(f["meas_words"], prog.num_measurements)
     fm = np.zeros((shots, prog.total_meas_slots), np.uint8)
     fm[:, :prog.num_measurements] = bits
-    a = cb.run(prog, shots, 0, precision="fp64", forced_meas=fm, trace=True)
-    b = cb.run(prog, shots, 0, precision="fp32", forced_meas=fm, trace=True)
-    pa, pb = np.nan_to_num(a["meas_prob"]), np.nan_to_num(b["meas_prob"])
-    return float(np.max(np.abs(pa - pb))) if pa.size else 0.0
+    ref = O.ref_forced(prog, fm)
+    out = {"program": name, "shots": shots}
+    for prec in ("fp32", "fp64"):
+        g = cb.run(prog, shots, 0, precision=prec, forced_meas=fm, trace=True)
+        out[f"{prec}_max_abs_prob_err"] = float(np.max(np.abs(np.nan_to_num(g["meas_prob"]) -
+                                                            np.nan_to_num(ref["meas_prob"])), initial=0.0))
+    hist, ops = prog.active_k_history(), prog.opcodes.tolist()
+    first = int(np.argmax(hist == prog.peak_rank))
+    cut = next((pc for pc in range(first, len(ops)) if ops[pc] in ACTIVE_MEAS), len(ops))
+    d = prog.to_npz_dict()
+    d["instructions"] = prog.instructions[:cut].copy()
+    pre = Program.from_npz_dict(d)
+    n = 2
+    f = cb.run(pre, n, 3, precision="fp64")
+    fm = np.zeros((n, pre.total_meas_slots), np.uint8)
+    fm[:, :pre.num_measurements] = cb.api._unpack(f["meas_words"], pre.num_measurements)
+    r = O.ref_forced(pre, fm)
+    k = int(r["final_k"][0])
+    ra = (r["final_gamma"][:, 0] + 1j * r["final_gamma"][:, 1])[:, None] * r["final_v"][:, :1 << k]
+    del r
+    for prec in ("fp32", "fp64"):
+        g = cb.run(pre, n, 0, precision=prec, forced_meas=fm, trace=True, dump_shots=n)
+        ga = (g["final_gamma"][:, 0] + 1j * g["final_gamma"][:, 1])[:, None] * g["final_v"][:, :1 << k]
+        del g
+        mx = rl2 = ov = 0.0
+        for s_ in range(n):
+            a_, b_ = ga[s_] / np.linalg.norm(ga[s_]), ra[s_] / np.linalg.norm(ra[s_])
+            mx = max(mx, float(np.abs(a_ - b_).max() / np.abs(b_).max()))
+            rl2 = max(rl2, float(np.linalg.norm(ga[s_] - ra[s_]) / np.linalg.norm(ra[s_])))
+            ov = max(ov, float(1.0 - abs(np.vdot(a_, b_))))
+        out[f"{prec}_amplitudes_at_k{k}"] = {"max_abs_err_rel_to_largest": mx, "rel_l2_err": rl2,
+                                            "one_minus_overlap": ov}
+        del ga
+    return out
 
 
 # ------------------------------------------------------------ CPU reference
@@ -357,25 +397,38 @@ def multi_program(torch, flush):
             "separate_launches_shots_per_s": total / (min(sep) / 1e3), "graph_over_separate": min(sep) / graph_ms}
 
 
+def literal_cfg3(torch, flush):
+    """The k = 24 program as its configuration states it: 10^3 shots per call
+    with at most 128 statevectors resident (16 GiB FP32), next to the default
+    residency (one wave: two CTAs on every SM)."""
+    prog = load_program(HEADLINE)
+    out = {"program": HEADLINE, "shots": 1000}
+    for key, cap in (("resident_128", 128), ("resident_one_wave", 0)):
+        r = time_device(torch, prog, 1000, "fp32", steps=2, warmup=1, rank=0, flush=flush, max_resident=cap)
+        out[f"{key}_shots_per_s"] = 1000 / (min(r["ms"]) / 1e3)
+    return out
+
+
 def gradients():
     """Adjoint d<P_j>/dphi_i on the rotation workload (n = 40, 32 rotations,
     16 probes redrawn on the active axes), 256 phase vectors."""
     import numpy as np
     from clifft_b200 import grad as GR
     from clifft_b200.workloads import active_probes
-    prog = active_probes(load_program("cfg4"))
+    base = load_program("cfg4")
     rng = np.random.default_rng(3)
-    phases = rng.uniform(0.0, 2 * np.pi, size=(256, GR.num_rot_params(prog)))
-    out = {"program": "cfg4 (n=40, 120 Clifford layers, 32 RZ, 16 probes on active axes), 256 phase vectors"}
-    for prec in ("fp64", "fp32"):
-        GR.expval_grad(prog, phases, precision=prec)
-        ts = []
-        for _ in range(3):
-            t0 = time.perf_counter()
+    phases = rng.uniform(0.0, 2 * np.pi, size=(256, GR.num_rot_params(base)))
+    out = {"program": "cfg4 (n=40, 120 Clifford layers, 32 RZ), 256 phase vectors"}
+    for label, prog in (("config_probes", base), ("active_probes", active_probes(base))):
+        for prec in ("fp64", "fp32"):
             GR.expval_grad(prog, phases, precision=prec)
-            ts.append(time.perf_counter() - t0)
-        out[f"{prec}_vectors_per_s"] = 256 / min(ts)
-        out[f"{prec}_ms_per_call"] = 1e3 * min(ts)
+            ts = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                GR.expval_grad(prog, phases, precision=prec)
+                ts.append(time.perf_counter() - t0)
+            out[f"{label}_{prec}_vectors_per_s"] = 256 / min(ts)
+            out[f"{label}_{prec}_ms_per_call"] = 1e3 * min(ts)
     return out
 
 
@@ -522,13 +575,15 @@ def main():
                 "program": "cfg1 (7x7 noisy memory grid, post-selected on all detectors)",
                 "shots": 1_000_000, "fp32_batched_shots_per_s": 1e9 / min(r1["ms"]),
                 "fp64_plain_shots_per_s": 1e9 / min(r1p["ms"]), "survivors_per_step": r1["passed"] / 2}
-            extras["max_abs_prob_diff_fp32_vs_fp64"] = {
-                "k24": prob_error(HEADLINE, 8), "k16": prob_error(extras["k_sweep"]["k16"]["program"], 64)}
+            extras["literal_cfg3"] = literal_cfg3(torch, flush)
             extras["multi_program_batch"] = multi_program(torch, flush)
             extras["expval_gradients"] = gradients()
             extras["sample_k"] = k_fault_sampling()
         if world == 1:
             cpu = cpu_baseline(HEADLINE)
+            if not args.no_extras:
+                extras["error_vs_reference"] = {
+                    "k24": reference_errors(HEADLINE, 4), "k16": reference_errors(extras["k_sweep"]["k16"]["program"], 16)}
     line = {
         "metric": METRIC,
         "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
@@ -541,8 +596,11 @@ def main():
         "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "note": f"algorithmic statevector bytes per launch / kernel time (peak {peak_kind}); "
-                             f"bytes actually streamed after fusion: {streamed_gbps:.0f} GB/s"},
+                     "dram_achieved": streamed_gbps, "dram_frac": streamed_gbps / peak,
+                     "note": f"achieved = algorithmic statevector bytes per launch (one pass per opcode, the "
+                             f"reference's algorithm) / kernel time; fused blocks stream fewer bytes, so it can "
+                             f"exceed the copy peak ({peak_kind}); dram_achieved = bytes actually streamed "
+                             f"(library counter, equal to ncu DRAM traffic within 3 %) / kernel time"},
         "e2e": e2e,
         "cpu_baseline": cpu,
         "extras": extras,

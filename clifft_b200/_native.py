@@ -36,7 +36,7 @@ class SampleArgs(ctypes.Structure):
     _fields_ = [
         ("shots", ctypes.c_uint64), ("seed", ctypes.c_uint64), ("first_shot", ctypes.c_uint64),
         ("precision", ctypes.c_uint32), ("flags", ctypes.c_uint32),
-        ("group_threads", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+        ("group_threads", ctypes.c_uint32), ("max_resident", ctypes.c_uint32),
         ("dust_eps", ctypes.c_double),
         ("forced_meas", P), ("fault_offsets", P), ("fault_sites", P), ("fault_channels", P),
         ("readout_offsets", P), ("readout_entries", P), ("stream", P),

@@ -88,7 +88,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
         profile: bool = False, autotune: bool = True, k_faults: Optional[int] = None,
-        segments: bool = True) -> Dict[str, object]:
+        segments: bool = True, max_resident: int = 0) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None / True = runs of
     consecutive opcodes share one pass over a global-memory statevector,
@@ -96,7 +96,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
     group_threads == 0, let the library time candidate launch shapes on the
     first large call and keep the fastest (False = fixed heuristic).
     `k_faults`: condition every shot on exactly that many fault events
-    (clifft_gpu_sample_k)."""
+    (clifft_gpu_sample_k). `max_resident`: at most this many statevectors
+    resident at once (0 = one full wave of the launch)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:
@@ -108,7 +109,7 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
     keep = []
     a = N.SampleArgs(shots=shots, seed=_seed(seed), first_shot=first_shot,
                      precision=_PRECISIONS[precision], group_threads=group_threads,
-                     dust_eps=dust_eps)
+                     dust_eps=dust_eps, max_resident=max_resident)
     flags = 0
     if survivors:
         flags |= N.CLIFFT_GPU_SURVIVORS

@@ -345,6 +345,13 @@ struct LaunchPlan {
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
 
+// CTA sizes (group_threads) of the warp-specialised CTA group: 256 or 512
+// threads compute on tiles, one more warp issues every bulk copy of a fused
+// block. The kernel instance fits in 96 registers, so two 288-thread CTAs
+// share an SM.
+constexpr uint32_t kWsThreads = 544, kWsThreadsHalf = 288;
+bool ws_shape(uint32_t threads) { return threads == kWsThreads || threads == kWsThreadsHalf; }
+
 // Shared-memory scratch of the tile engine for one shot group.
 uint32_t tile_scratch_bytes(uint32_t precision, bool cta, uint32_t stages) {
     if (precision == CLIFFT_GPU_FP32)
@@ -396,10 +403,16 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
     L.G = G;
     L.S = G ? 32 / G : 1;
     L.nw_words = nw_template(p.meta.num_words);
-    L.fn = precision == CLIFFT_GPU_FP32 ? kernel_f32(G, int(L.nw_words)) : kernel_f64(G, int(L.nw_words));
-    cudaFuncAttributes fa{};
-    CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
-    const int max_threads = std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
+    // a CTA of 288 / 544 threads: 256 / 512 compute threads and one warp
+    // that only moves the fused blocks' tiles (the warp-specialised kernel
+    // instance, G = -1); the size is settled below for automatic requests
+    auto pick_fn = [&](int kg) {
+        L.fn = precision == CLIFFT_GPU_FP32 ? kernel_f32(kg, int(L.nw_words)) : kernel_f64(kg, int(L.nw_words));
+        cudaFuncAttributes fa{};
+        CUDA_OK(cudaFuncGetAttributes(&fa, (const void*)L.fn));
+        return std::max(32, (fa.maxThreadsPerBlock / 32) * 32);
+    };
+    int max_threads = pick_fn(G);
     // one-shot groups (a CTA, or a warp of 32 lanes) stream global
     // statevectors through the tile engine: two 4 KiB buffers per warp keep
     // sixteen warps per SM (three buffers, twelve warps: 10 % slower at k = 14..17)
@@ -426,11 +439,15 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
         }
     } else {
         // default: 128 threads (three CTAs with two tile buffers each share an
-        // SM) up to 8 MiB statevectors, else 256 (two CTAs, three buffers)
-        int t = group_req > 32 ? int(group_req) : (state_bytes <= (size_t(8) << 20) ? 128 : 256);
+        // SM) up to 8 MiB statevectors, else two CTAs with three buffers each:
+        // 256 compute threads plus a copy warp when blocks fuse (k = 24: 98 vs
+        // 107 ms), 256 threads without fusion
+        int t = group_req > 32 ? int(group_req)
+                               : (state_bytes <= (size_t(8) << 20) ? 128 : (allow_fusion ? int(kWsThreadsHalf) : 256));
+        if (ws_shape(uint32_t(t))) max_threads = pick_fn(-1);
         L.threads = std::min(t, max_threads);
         L.regions = 1;
-        L.stages = L.threads <= 128 ? 2 : (L.threads <= 256 ? 3 : 4);
+        L.stages = L.threads <= 128 ? 2 : (L.threads <= 256 || L.threads == int(kWsThreadsHalf) ? 3 : 4);
         L.state_in_smem = region_bytes(true) + tail(L.threads) <= smem_cap;
     }
     L.tiles = (G == 0 || G == 32) && !L.state_in_smem;
@@ -500,7 +517,7 @@ void keep_pool_memory(int dev) {
 // the device queries; the grid is sized per call.
 LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
                        uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words,
-                       bool allow_fusion) {
+                       bool allow_fusion, uint32_t max_resident = 0) {
     const auto key = std::make_tuple(precision, group_req, allow_fusion, rec_words, det_words, obs_words);
     PlanShape ps;
     {
@@ -530,6 +547,7 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         uint64_t max_blocks = std::max<uint64_t>(1, (free_b / 2) / std::max<uint64_t>(per_block_bytes, 1));
         blocks = std::min<uint64_t>(blocks, max_blocks);
     }
+    if (max_resident) blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, max_resident / shots_per_block));
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, blocks_needed));
     L.blocks = int(blocks);
     return L;
@@ -539,7 +557,8 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
 // around the heuristic width for shared-memory statevectors, warp or CTA
 // groups for L2/HBM-resident ones up to 4 MiB, and for larger statevectors
 // CTAs of 128 (two tile buffers, three CTAs per SM), 256 (three buffers, two
-// per SM) or 512 threads (four buffers).
+// per SM), 512 threads (four buffers) or 256 / 512 + a copy warp (three /
+// four buffers, warp-specialised fused blocks).
 std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t precision) {
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const size_t state_bytes = (size_t(1) << p.meta.peak_rank) * amp;
@@ -551,7 +570,7 @@ std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t prec
     } else if (state_bytes <= (size_t(4) << 20)) {
         c = {32, 16, 64, 128, 256};
     } else {
-        c = {128, 256, 512};
+        c = {128, 256, 512, kWsThreadsHalf, kWsThreads};
     }
     return c;
 }
@@ -902,7 +921,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             }
         }
         LaunchPlan L = plan_launch(*prog, args->precision, group_req, shots, rec_words, det_words, obs_words,
-                                   allow_fusion);
+                                   allow_fusion, args->max_resident);
         KParams K{};
         K.shots = shots;
         K.first_shot = args->first_shot;
@@ -1018,7 +1037,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             uint32_t best = 0;
             for (uint32_t cand : tune) {
                 LaunchPlan Lc = plan_launch(*prog, args->precision, cand, shots, rec_words, det_words, obs_words,
-                                            allow_fusion);
+                                            allow_fusion, args->max_resident);
                 const uint64_t wave = uint64_t(Lc.blocks) * Lc.regions * Lc.S;
                 const uint64_t trial = std::min<uint64_t>(shots, 2 * wave);
                 KParams Kc = K;
@@ -1050,7 +1069,8 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
                 g_tuned[tune_id] = best;
                 tune_file_store(prog->content_hash, prog->device, tune_key, best);
             }
-            L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion);
+            L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion,
+                            args->max_resident);
         }
         apply_plan(K, L);
         // Survivor runs of warp groups go segment by segment: the program is cut
@@ -1391,7 +1411,8 @@ int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_s
                 auto f = g_tuned.find(std::make_tuple(p->content_hash, p->device, key));
                 if (f != g_tuned.end()) group_req = f->second;
             }
-            it.L = plan_launch(*p, a.precision, group_req, a.shots, rec_words, det_words, obs_words, allow_fusion);
+            it.L = plan_launch(*p, a.precision, group_req, a.shots, rec_words, det_words, obs_words, allow_fusion,
+                               a.max_resident);
             KParams& K = it.K;
             K.shots = a.shots;
             K.first_shot = a.first_shot;

@@ -13,6 +13,7 @@ KernelFn pick_by_group(int G) {
         case 8: return svm_sample_kernel<R, 8, NW>;
         case 16: return svm_sample_kernel<R, 16, NW>;
         case 32: return svm_sample_kernel<R, 32, NW>;
+        case -1: return svm_sample_kernel<R, -1, NW>;
         default: return svm_sample_kernel<R, 0, NW>;
     }
 }

@@ -283,6 +283,7 @@ __device__ __forceinline__ double philox_uniform(uint64_t seed, uint64_t shot, u
 template <int G>
 struct Lanes {
     static constexpr bool kCta = false;
+    static constexpr bool kWS = false;
     static constexpr int S = 32 / G;
     __device__ static __forceinline__ int size() { return G; }
     __device__ static __forceinline__ int rank() { return (int)(threadIdx.x & 31) & (G - 1); }
@@ -297,6 +298,7 @@ struct Lanes {
 // A whole CTA per shot.
 struct CtaLanes {
     static constexpr bool kCta = true;
+    static constexpr bool kWS = false;
     static constexpr int S = 1;
     __device__ static __forceinline__ int size() { return blockDim.x; }
     __device__ static __forceinline__ int rank() { return threadIdx.x; }
@@ -311,6 +313,15 @@ struct GroupOf {
 template <>
 struct GroupOf<0> {
     using type = CtaLanes;
+};
+// A whole CTA per shot whose last warp only moves tiles in fused blocks
+// (warp-specialised tile engine); every other step runs on all its threads.
+struct CtaLanesWS : CtaLanes {
+    static constexpr bool kWS = true;
+};
+template <>
+struct GroupOf<-1> {
+    using type = CtaLanesWS;
 };
 
 __device__ __forceinline__ uint64_t ins0(uint64_t v, uint32_t pos) {
@@ -452,15 +463,16 @@ constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 // fuses up to 24 opcodes per pass; a warp running one shot streams 4 KiB
 // tiles through two buffers and fuses up to 24 (FP32) / 16 (FP64), which
 // leaves room for four 4-warp CTAs per SM (the register limit). Scratch
-// layout of one group: [kMaxStages mbarriers][micro-ops][64 run offsets]
-// [64-byte axis -> local bit table][stages tile buffers, 128-B aligned].
+// layout of one group: [2 x kMaxStages mbarriers: tile loaded / tile computed]
+// [micro-ops][64 run offsets][64-byte axis -> local bit table]
+// [stages tile buffers, 128-B aligned].
 template <typename R, bool CTA>
 struct TileCfg {
     using MOp = MicroOpT<typename Cx<R>::T>;
     static constexpr int kBits = CTA ? (sizeof(R) == 4 ? 12 : 11) : (sizeof(R) == 4 ? 9 : 8);
     static constexpr int kMops = CTA ? 24 : (sizeof(R) == 4 ? 24 : 16);
     static constexpr uint32_t kBarOffset = 0;
-    static constexpr uint32_t kMopsOffset = kMaxStages * 8u;
+    static constexpr uint32_t kMopsOffset = 2u * kMaxStages * 8u;
     static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MOp);
     static constexpr uint32_t kLbitOffset = kTablesOffset + 64u * 8u;
     static constexpr uint32_t kBufOffset = (kLbitOffset + 64u + 127u) & ~127u;
@@ -505,6 +517,21 @@ __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+// barrier 1 over the first n threads of the CTA (the compute warps of a
+// warp-specialised CTA group; barrier 0 is __syncthreads)
+__device__ __forceinline__ void bar_sync_first(uint32_t n) { asm volatile("bar.sync 1, %0;\n" ::"r"(n) : "memory"); }
+__device__ __forceinline__ bool bar_or_first(uint32_t n, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.cta.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(n)
+        : "memory");
+    return r != 0;
+}
 __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
@@ -938,6 +965,18 @@ struct Shot {
         } else {
             phase_sweep(a, zr, zi);
         }
+    }
+    // Barrier of the threads that compute on tiles in a fused block: the
+    // whole group, or every warp but the copy warp of a warp-specialised CTA.
+    // threads that compute on tiles in a fused block
+    static __device__ __forceinline__ int compute_threads() {
+        return Grp::kWS ? (int)blockDim.x - 32 : Grp::size();
+    }
+    static __device__ __forceinline__ void csync() {
+        if constexpr (Grp::kWS)
+            bar_sync_first(blockDim.x - 32u);
+        else
+            Grp::sync();
     }
     // Statevector passes of a one-shot group with a global-memory statevector
     // larger than one tile go through the bulk-copy tile engine.
@@ -1833,6 +1872,144 @@ struct Shot {
         return ok_all;
     }
 
+    // The same pass for a warp-specialised CTA group (fused blocks only;
+    // loads from and stores to the same logical tiles): the last warp issues
+    // every bulk load and store, the other warps only wait for loaded stages
+    // and compute. Each stage has two mbarriers: `full` (the load's bytes
+    // arrived) and `done` (the compute warps finished the tile; thread 0
+    // arrives once). The copy warp refills a stage when its tile is done and
+    // the tile's store has read the buffer, while the compute warps move on
+    // to the next loaded stage. Every wait is bounded; a timeout on either
+    // side is agreed on by the whole CTA, which drains its loads and stops.
+    // In a completed pass every stage's two barriers complete once per tile
+    // mapped to it, so every thread advances its copy of the phase bits the
+    // same way.
+    template <class Compute>
+    __device__ bool stream_tiles_ws(uint64_t ntiles, uint64_t C, uint32_t r, uint32_t store_runs, uint32_t skip,
+                                    Compute compute) {
+        constexpr uint32_t MB = TC::kBits;
+        constexpr uint32_t TN = 1u << MB;
+        T* bufs = reinterpret_cast<T*>(fuse + TC::kBufOffset);
+        uint64_t* full = reinterpret_cast<uint64_t*>(fuse + fuse_bar_offset());
+        uint64_t* done = full + kMaxStages;
+        const uint32_t nst = K.stages;
+        const uint64_t* runoff = reinterpret_cast<const uint64_t*>(fuse + fuse_tables_offset());
+        const uint32_t nruns = 1u << (MB - r);
+        const uint32_t run_bytes = (1u << r) * (uint32_t)sizeof(T);
+        const uint32_t load_bytes = (nruns >> __popc(skip)) * run_bytes;
+        const uint64_t lx = xo;
+        const uint32_t ncomp = blockDim.x - 32u;
+        const bool copier = threadIdx.x >= ncomp;
+        const uint32_t lane = threadIdx.x & 31u;
+        uint32_t phase = *bar_phase;  // bits 0..3: full parity per stage, 8..11: done parity, 31: dead
+        if (phase >> 31) {
+            stop = true;
+            return false;
+        }
+        auto next_base = [C](uint64_t b) { return ((b | ~C) + 1) & C; };
+        // statevector writes made by ordinary stores must be visible to the copy engine
+        fence_async_global();
+        __syncthreads();
+        bool ok = true;
+        uint64_t t = 0;
+        uint32_t loads[kMaxStages] = {0, 0, 0, 0};  // loads issued per stage (copy warp)
+        long long waited = 0;
+        if (copier) {
+            uint64_t lbase = 0, lt = 0;
+            auto load = [&](uint32_t st) {
+                if (lane == 0) mbar_expect_tx(&full[st], load_bytes);
+                __syncwarp();
+                for (uint32_t j = lane; j < nruns; j += 32)
+                    if (!(j & skip))
+                        bulk_load(bufs + st * TN + (j << r), v + ((lbase + runoff[j]) ^ lx), run_bytes, &full[st]);
+                loads[st]++;
+                lbase = next_base(lbase);
+                ++lt;
+            };
+            for (uint32_t st = 0; st < nst && lt < ntiles; ++st) load(st);
+            uint64_t sbase = 0;
+            uint32_t st = 0;
+            for (; t < ntiles; ++t, st = st + 1 == nst ? 0 : st + 1) {
+                const uint32_t parity = (phase >> (8 + st)) & 1u;
+                uint32_t got = 0;
+                const long long w0 = clock64();
+                for (uint32_t it = 0; it < (1u << 20) && !got; ++it) got = mbar_try_wait(&done[st], parity);
+                waited = clock64() - w0;
+                if (__any_sync(0xffffffffu, !got)) {
+                    ok = false;
+                    break;
+                }
+                phase ^= 1u << (8 + st);
+                if (store_runs) {
+                    for (uint32_t j = lane; j < store_runs; j += 32)
+                        bulk_store(v + ((sbase + runoff[j]) ^ lx), bufs + st * TN + (j << r), run_bytes);
+                    bulk_commit();
+                }
+                sbase = next_base(sbase);
+                if (lt < ntiles) {  // tile t + nst into this stage once its store has read it
+                    if (store_runs) bulk_wait_read0();
+                    __syncwarp();
+                    load(st);
+                }
+            }
+            bulk_wait_all();
+            fence_async_global();
+        } else {
+            uint64_t tbase = 0;
+            uint32_t st = 0;
+            for (; t < ntiles; ++t, tbase = next_base(tbase), st = st + 1 == nst ? 0 : st + 1) {
+                const uint32_t parity = (phase >> st) & 1u;
+                uint32_t got = 0;
+                const long long w0 = clock64();
+                for (uint32_t it = 0; it < (1u << 20) && !got; ++it) got = mbar_try_wait(&full[st], parity);
+                waited = clock64() - w0;
+                if (bar_or_first(ncomp, !got)) {
+                    ok = false;
+                    break;
+                }
+                phase ^= 1u << st;
+                compute(bufs + st * TN, t, tbase);  // ends with a compute-warp barrier
+                // the tile's writes before the copy warp's bulk store reads them
+                fence_async_shared();
+                bar_sync_first(ncomp);
+                if (threadIdx.x == 0) mbar_arrive(&done[st]);
+            }
+        }
+        const bool failed = __syncthreads_or(!ok) != 0;
+        if (!failed) {
+            // every stage's barriers completed once per tile mapped to it
+            phase = *bar_phase;
+            for (uint32_t st = 0; st < nst; ++st)
+                if (((ntiles + nst - 1 - st) / nst) & 1u) phase ^= (1u << st) | (1u << (8 + st));
+        } else {
+            if (threadIdx.x == 0 && atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT) == 0 && K.error_info) {
+                K.error_info[0] = cur_site;
+                K.error_info[1] = cur_pc;
+                K.error_info[2] = t;
+                K.error_info[3] = ntiles;
+                K.error_info[4] = r;
+                K.error_info[5] = k;
+                K.error_info[6] = 1000 + (unsigned long long)copier;
+                K.error_info[7] = (unsigned long long)waited;
+            }
+            if (copier) {
+                // wait (bounded) for the last load issued into each stage
+                const uint32_t p0 = *bar_phase;
+                for (uint32_t st = 0; st < nst; ++st) {
+                    if (!loads[st]) continue;
+                    const uint32_t par = ((p0 >> st) ^ (loads[st] - 1u)) & 1u;
+                    for (uint32_t it = 0; it < (1u << 20); ++it)
+                        if (mbar_try_wait(&full[st], par)) break;
+                }
+            }
+            phase |= 1u << 31;
+            stop = true;
+        }
+        *bar_phase = phase;
+        __syncthreads();
+        return !failed;
+    }
+
     // The same pass for a warp running one shot: two 4 KiB buffers filled by
     // 16-byte asynchronous copies from every lane (cp.async, waited for per
     // lane, then a warp barrier) and written back with 16-byte stores. Bulk
@@ -2026,10 +2203,10 @@ struct Shot {
         resolving = false;
         if (Grp::rank() == 0)
             compile_index_runs(reinterpret_cast<MOp*>(fuse + fuse_mops_offset()), n_mops,
-                               (1u << MB) / (uint32_t)Grp::size());
+                               (1u << MB) / (uint32_t)compute_threads());
         Grp::sync();
         const MOp* mops = reinterpret_cast<const MOp*>(fuse + fuse_mops_offset());
-        const int tid = Grp::rank(), nthr = Grp::size();
+        const int tid = Grp::rank(), nthr = compute_threads();
         const int nm = n_mops;
         cur_site = 6;
         constexpr uint32_t TN = 1u << MB;
@@ -2039,7 +2216,7 @@ struct Shot {
         // an X-basis terminator's H is the block's last micro-op: applied
         // together with the half-norm sums
         const int nmo = term_kind >= 2 ? nm - 1 : nm;
-        stream_tiles(1ull << (kk - MB), C, r, 0, 0, nm ? nruns : 0, skip, [&](T* buf, uint64_t, uint64_t tbase) {
+        auto body = [&](T* buf, uint64_t, uint64_t tbase) {
             for (int j = 0; j < nmo;) {
                 int e = j;
                 while (e < nmo && index_map_kind(mops[e].kind)) ++e;
@@ -2054,7 +2231,7 @@ struct Shot {
                     continue;
                 }
                 apply_micro(mops[j], buf, tid, nthr, tbase);
-                Grp::sync();
+                csync();
                 ++j;
             }
             if (term_kind >= 2) {
@@ -2094,8 +2271,12 @@ struct Shot {
                 acc[0] += q0;
                 acc[1] += q1;
             }
-            Grp::sync();
-        });
+            csync();
+        };
+        if constexpr (Grp::kWS)
+            stream_tiles_ws(1ull << (kk - MB), C, r, nm ? nruns : 0, skip, body);
+        else
+            stream_tiles(1ull << (kk - MB), C, r, 0, 0, nm ? nruns : 0, skip, body);
         moved += (((1ull << kk) >> __popcll(fresh)) + (nm ? (1ull << kk) : 0ull)) * sizeof(T);
         if (term_kind) {
             group_reduce<Grp, 2>(acc, red);
@@ -2265,7 +2446,7 @@ struct Shot {
         uint32_t cq[QB];
 #pragma unroll
         for (uint32_t i = 0; i < QB; ++i) cq[i] = fc[lg + i];
-        Grp::sync();
+        csync();
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
             uint32_t pq = lt;
@@ -2274,7 +2455,7 @@ struct Shot {
                 if ((q >> i) & 1) pq ^= cq[i];
             tile[pq] = v[q];
         }
-        Grp::sync();
+        csync();
     }
 
     // One micro-op on a shared-memory tile of 2^TILE_BITS amplitudes whose
@@ -2795,11 +2976,12 @@ struct Shot {
 // broadcast slot.
 template <int G>
 __host__ __device__ constexpr int shots_per_group_region() {
-    return G == 0 ? 1 : 32 / G;
+    return G <= 0 ? 1 : 32 / G;
 }
 
 template <typename R, int G, int NW>
-__global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample_kernel(const DevProg P, const KParams K) {
+__global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1 : 4)
+    svm_sample_kernel(const DevProg P, const KParams K) {
     using Grp = typename GroupOf<G>::type;
     using T = typename Cx<R>::T;
     constexpr int S = Grp::S;
@@ -2825,7 +3007,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : 128, G == 0 ? 1 : 4) svm_sample
         // group runs
         if (Grp::rank() == 0) {
             uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW>::fuse_bar_offset());
-            for (int st = 0; st < kMaxStages; ++st) mbar_init(&bars[st], 1);
+            for (int st = 0; st < 2 * kMaxStages; ++st) mbar_init(&bars[st], 1);
             mbar_fence_init();
         }
         __syncthreads();

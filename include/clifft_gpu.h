@@ -82,8 +82,11 @@ typedef struct clifft_gpu_sample_args {
     uint32_t precision;     /* CLIFFT_GPU_FP64 or CLIFFT_GPU_FP32 */
     uint32_t flags;
     uint32_t group_threads; /* 0 = automatic (autotuned, see below); 1,2,4..32 = lanes per shot
-                               (32/G shots per warp); 64..1024 = one CTA of that size per shot */
-    uint32_t reserved;
+                               (32/G shots per warp); 64..1024 = one CTA of that size per shot;
+                               288 / 544 = one CTA of 256 / 512 compute threads plus a warp that
+                               issues the tile copies of fused blocks */
+    uint32_t max_resident;  /* upper bound on shots whose statevectors are resident at once (shots run
+                               in waves of at most this many); 0 = as many as one wave of the launch holds */
     double dust_eps;        /* relative dust threshold; 0 = 1e-18 (FP64) / 1e-9 (FP32) */
     /* CLIFFT_GPU_FORCED_MEAS: shots x total_meas_slots bytes (0/1) */
     const uint8_t* forced_meas;

@@ -2,7 +2,7 @@
 oracle run of the same size:
 
   * k = 24 (2^24 amplitudes per shot): under forced outcomes every launch
-    shape (128 / 256 / 512-thread CTAs) and fused vs one-pass-per-opcode
+    shape (128 / 256 / 512-thread CTAs, 256 / 512 + a copy warp) and fused vs one-pass-per-opcode
     execution give the same records and FP64 probabilities to 1e-12, and the
     FP32 statevector stays within 1e-5 of FP64 on every probability;
   * the 10^6-shot post-selected memory grid: the survivor fraction and the
@@ -45,7 +45,7 @@ def test_k24_shapes_fusion_and_precision():
     assert prog.peak_rank == 24
     fm = _forced(prog, 4, 9)
     runs = {}
-    for group in (128, 256, 512):
+    for group in (128, 256, 288, 512, 544):
         for fusion in (True, False):
             if group != 256 and not fusion:
                 continue

@@ -129,7 +129,7 @@ def test_launch_shape_independence(group):
                                amplitudes(ref["final_gamma"], ref["final_v"]), atol=1e-10)
 
 
-@pytest.mark.parametrize("group", [32, 128, 256, 512])
+@pytest.mark.parametrize("group", [32, 128, 256, 288, 512, 544])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_large_k_global_state_forced_parity(precision, group):
     # k = 17: 2^17 amplitudes per shot in a global slab, one warp per shot
@@ -222,7 +222,7 @@ def test_record_probabilities_match_oracle():
     np.testing.assert_allclose(lp[reach], f["log_prob"][reach], atol=1e-10)
 
 
-@pytest.mark.parametrize("group", [32, 128, 256, 512])
+@pytest.mark.parametrize("group", [32, 128, 256, 288, 512, 544])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_fused_tile_sweeps_match_unfused(precision, group):
     # k = 16 with the reference's U2 / U4 / MULTI nodes: fused blocks perform
@@ -236,7 +236,9 @@ def test_fused_tile_sweeps_match_unfused(precision, group):
     # probabilities and gamma agree to FP64 rounding in FP64 (1e-13) and to
     # 1e-8 in FP32.
     # (A warp per shot streams 4 KiB tiles through two buffers, 128 / 256 /
-    # 512-thread CTAs 32 KiB tiles through two / three / four.)
+    # 512-thread CTAs 32 KiB tiles through two / three / four; 288 / 544-thread
+    # CTAs compute with 256 / 512 threads while their last warp issues the
+    # copies.)
     prog, d = load_case(os.path.join(os.path.dirname(__file__), "golden", "fuzz_k16.npz"))
     fm = d["forced_meas_in"]
     faults, ros = unflatten(d)
@@ -259,3 +261,15 @@ def test_fused_tile_sweeps_match_unfused(precision, group):
     fa = cb.run(prog, 64, 3, precision=precision, fusion=True)
     fb = cb.run(prog, 64, 3, precision=precision, fusion=False)
     assert np.array_equal(fa["meas_words"], fb["meas_words"])
+
+
+def test_resident_cap_gives_the_same_records():
+    # max_resident bounds the statevectors held at once (shots then run in
+    # waves); per-shot Philox streams make the records independent of it
+    prog = O.ref_passes(random_program(7, n=20, length=170, max_k=17, noise=False, classical=False,
+                                       expand_bias=0.5), O.PASS_ALL) if O.ref_available() else \
+        random_program(7, n=20, length=170, max_k=17, noise=False, classical=False, expand_bias=0.5)
+    a = cb.run(prog, 600, 9, precision="fp64", group_threads=256)
+    b = cb.run(prog, 600, 9, precision="fp64", group_threads=256, max_resident=40)
+    assert np.array_equal(a["meas_words"], b["meas_words"])
+    np.testing.assert_allclose(a["exp_vals"], b["exp_vals"], atol=1e-12)
