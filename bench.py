@@ -118,14 +118,14 @@ class ClockSampler:
 
 # ------------------------------------------------------------ GPU helpers
 def device_run(dp, shots, seed, first_shot, precision, stream, bufs, survivors=False, plain=False, group=0,
-               max_resident=0):
+               max_resident=0, extra_flags=0):
     """One device-resident sampling step: program resident, outputs in HBM.
     plain = the plain executor: one pass per opcode, fixed heuristic launch
     shape, one launch per call (no fusion, no autotuning, no survivor
-    compaction)."""
+    compaction). extra_flags: further CLIFFT_GPU_* flags (e.g. TENSOR_DENSE)."""
     import ctypes
     from clifft_b200 import _native as N
-    flags = N.CLIFFT_GPU_DEVICE_PTRS
+    flags = N.CLIFFT_GPU_DEVICE_PTRS | extra_flags
     if survivors:
         flags |= N.CLIFFT_GPU_SURVIVORS
     if plain:
@@ -154,7 +154,7 @@ def output_buffers(torch, prog, shots, dev):
 
 
 def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survivors=False, plain=False,
-                group=0, max_resident=0):
+                group=0, max_resident=0, extra_flags=0):
     import clifft_b200 as cb
     dev = torch.device("cuda", torch.cuda.current_device())
     dp = cb.load(prog)
@@ -162,14 +162,16 @@ def time_device(torch, prog, shots, precision, steps, warmup, rank, flush, survi
     bufs = output_buffers(torch, prog, shots, dev)
     first = rank * shots
     for w in range(warmup):
-        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain, group, max_resident)
+        device_run(dp, shots, 1000 + w, first, precision, stream, bufs, survivors, plain, group, max_resident,
+                   extra_flags)
     torch.cuda.synchronize()
     times, kernel_ms, launches, passed, alg_bytes, streamed, groups = [], [], 0, 0, 0, 0, set()
     for s in range(steps):
         flush.zero_()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
-        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain, group, max_resident)
+        o = device_run(dp, shots, 7 + s, first, precision, stream, bufs, survivors, plain, group, max_resident,
+                       extra_flags)
         ev1.record(stream)
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1))
@@ -409,6 +411,24 @@ def literal_cfg3(torch, flush):
     return out
 
 
+def dense_blocks(torch, flush):
+    """The dense k = 20 program (U2 / U4 / H runs; peak 2^20 amplitudes, FP32)
+    with its dense blocks on the tensor cores (3xTF32 MMAs) and on the CUDA
+    cores: kernel-time shots/s of each and their ratio. The configured
+    programs form no dense block, so the flag does not change them."""
+    from clifft_b200 import _native as N
+    prog = load_program("dense_k20")
+    shots = 592  # four waves of two CTAs on every SM
+    out = {"program": "dense_k20", "peak_k": prog.peak_rank, "shots": shots, "group_threads": 288}
+    for key, fl in (("tensor_cores", N.CLIFFT_GPU_TENSOR_DENSE), ("cuda_cores", 0)):
+        r = time_device(torch, prog, shots, "fp32", steps=3, warmup=3, rank=0, flush=flush, group=288,
+                        extra_flags=fl)
+        out[f"{key}_shots_per_s"] = shots / (min(r["kernel_ms"]) / 1e3)
+        out[f"{key}_kernel_ms"] = min(r["kernel_ms"])
+    out["tensor_over_cuda_cores"] = out["tensor_cores_shots_per_s"] / out["cuda_cores_shots_per_s"]
+    return out
+
+
 def gradients():
     """Adjoint d<P_j>/dphi_i on the rotation workload (n = 40, 32 rotations,
     16 probes redrawn on the active axes), 256 phase vectors."""
@@ -463,16 +483,21 @@ def main():
     ap.add_argument("--plain", action="store_true", help="with --profile: the plain executor")
     ap.add_argument("--group", type=int, default=0,
                     help="with --profile: fixed group_threads (no autotuning trial launches)")
+    ap.add_argument("--tensor-dense", action="store_true",
+                    help="with --profile: dense blocks of fused sweeps on the tensor cores")
     args = ap.parse_args()
     if args.profile:
         import torch
         torch.cuda.set_device(0)
         prog = load_program(args.profile)
         flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+        from clifft_b200 import _native as N
         r = time_device(torch, prog, args.shots, args.precision, args.steps, args.warmup, 0, flush,
-                        survivors=bool(prog.has_postselection), plain=args.plain, group=args.group)
+                        survivors=bool(prog.has_postselection), plain=args.plain, group=args.group,
+                        extra_flags=N.CLIFFT_GPU_TENSOR_DENSE if args.tensor_dense else 0)
         print(json.dumps({"program": args.profile, "shots": args.shots, "precision": args.precision,
-                          "plain": args.plain, "ms": r["ms"], "kernel_ms": r["kernel_ms"],
+                          "plain": args.plain, "tensor_dense": args.tensor_dense,
+                          "ms": r["ms"], "kernel_ms": r["kernel_ms"],
                           "alg_bytes": r["alg_bytes"], "streamed_bytes": r["streamed_bytes"],
                           "launches": r["launches"], "group_threads": r["group_threads"]}))
         return
@@ -576,6 +601,7 @@ def main():
                 "shots": 1_000_000, "fp32_batched_shots_per_s": 1e9 / min(r1["ms"]),
                 "fp64_plain_shots_per_s": 1e9 / min(r1p["ms"]), "survivors_per_step": r1["passed"] / 2}
             extras["literal_cfg3"] = literal_cfg3(torch, flush)
+            extras["dense_blocks"] = dense_blocks(torch, flush)
             extras["multi_program_batch"] = multi_program(torch, flush)
             extras["expval_gradients"] = gradients()
             extras["sample_k"] = k_fault_sampling()

@@ -9,16 +9,17 @@ include/clifft_gpu.h:
     res = cb.sample_survivors(program, 10**6, keep_records=True)  # clifft.sample_survivors
     lp  = cb.record_probabilities(program, records)            # clifft.record_probabilities
     res = cb.sample_k(program, shots=10**5, k=2)                # clifft.sample_k
+    ref = cb.compute_reference_syndrome(program)                # clifft.compute_reference_syndrome
 """
 
 from .program import OP, OPCODES, Program
 from ._sample_result import SampleResult
-from .api import (DeviceProgram, load, noise_site_probabilities, record_probabilities, run, sample,
-                  sample_k, sample_k_survivors, sample_survivors)
+from .api import (DeviceProgram, compute_reference_syndrome, load, noise_site_probabilities,
+                  record_probabilities, run, sample, sample_k, sample_k_survivors, sample_survivors)
 from ._native import backend_name
 
 __all__ = [
     "OP", "OPCODES", "Program", "SampleResult", "DeviceProgram", "load", "run", "sample",
     "sample_survivors", "sample_k", "sample_k_survivors", "noise_site_probabilities",
-    "record_probabilities", "backend_name",
+    "record_probabilities", "compute_reference_syndrome", "backend_name",
 ]

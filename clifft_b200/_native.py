@@ -26,6 +26,8 @@ CLIFFT_GPU_FORCE_FUSION = 0x40
 CLIFFT_GPU_PROFILE = 0x80
 CLIFFT_GPU_NO_AUTOTUNE = 0x100
 CLIFFT_GPU_NO_SEGMENTS = 0x200
+CLIFFT_GPU_RAW_PARITY = 0x400
+CLIFFT_GPU_TENSOR_DENSE = 0x800
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "device error", -4: "out of memory"}
 

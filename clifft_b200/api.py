@@ -88,7 +88,8 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         dump_shots: int = 0, group_threads: int = 0, first_shot: int = 0,
         dust_eps: float = 0.0, want_records: bool = True, fusion: Optional[bool] = None,
         profile: bool = False, autotune: bool = True, k_faults: Optional[int] = None,
-        segments: bool = True, max_resident: int = 0) -> Dict[str, object]:
+        segments: bool = True, max_resident: int = 0, raw_parity: bool = False,
+        tensor_dense: bool = False) -> Dict[str, object]:
     """Low-level call of clifft_gpu_sample with host buffers; returns packed
     records plus everything the call reports. `fusion`: None / True = runs of
     consecutive opcodes share one pass over a global-memory statevector,
@@ -97,7 +98,11 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
     first large call and keep the fastest (False = fixed heuristic).
     `k_faults`: condition every shot on exactly that many fault events
     (clifft_gpu_sample_k). `max_resident`: at most this many statevectors
-    resident at once (0 = one full wave of the launch)."""
+    resident at once (0 = one full wave of the launch). `raw_parity`:
+    detectors / observables without their expected parities and POSTSELECT
+    recorded instead of discarding (CLIFFT_GPU_RAW_PARITY). `tensor_dense`:
+    FP32 dense blocks of fused sweeps on the tensor cores
+    (CLIFFT_GPU_TENSOR_DENSE)."""
     if precision not in _PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
     if shots < 0:
@@ -136,6 +141,10 @@ def run(program: Program, shots: int, seed: Optional[int] = None, *, precision: 
         flags |= N.CLIFFT_GPU_NO_AUTOTUNE
     if not segments:
         flags |= N.CLIFFT_GPU_NO_SEGMENTS
+    if raw_parity:
+        flags |= N.CLIFFT_GPU_RAW_PARITY
+    if tensor_dense:
+        flags |= N.CLIFFT_GPU_TENSOR_DENSE
     if fusion is False:
         flags |= N.CLIFFT_GPU_NO_FUSION
     elif fusion is True:
@@ -235,6 +244,23 @@ def _survivor_result(p: Program, r: Dict[str, object], keep_records: bool, shots
     return SampleResult(meas, det, obs, total_shots=int(shots), passed_shots=r["passed_shots"],
                         logical_errors=r["logical_errors"], observable_ones=r["observable_ones"],
                         exp_vals=ev, stats=_stats(r))
+
+
+def compute_reference_syndrome(program: Program, *, precision: str = "fp64") -> Dict[str, np.ndarray]:
+    """Noiseless reference syndrome: the detector and observable parities of
+    one noise-free shot with seed 0 (clifft::compute_reference_syndrome,
+    src/clifft/api/reference_syndrome.cc:9-30), which the reference uses to
+    normalise syndromes. The reference strips the noise from its HIR and
+    lowers again without post-selection or expected parities; on the
+    compiled program the same shot runs with every noise site and readout
+    flip switched off (forced-fault mode with no faults), detectors and
+    observables without their expected parities, and POSTSELECT instructions
+    recorded in their detector slots instead of discarding. Returns
+    {"detectors": uint8[num_detectors], "observables": uint8[num_observables]}."""
+    p = program
+    r = run(p, 1, 0, precision=precision, faults=[[]], readout_faults=[[]], raw_parity=True)
+    return {"detectors": _unpack(r["det_words"], p.num_detectors)[0].copy(),
+            "observables": _unpack(r["obs_words"], p.num_observables)[0].copy()}
 
 
 def record_probabilities(program: Program, records: np.ndarray, *,

@@ -929,7 +929,9 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         K.dust_eps = args->dust_eps > 0.0 ? args->dust_eps : (args->precision == CLIFFT_GPU_FP32 ? 1e-9 : 1e-18);
         K.flags = (args->flags & CLIFFT_GPU_SURVIVORS ? KF_SURVIVORS : 0) |
                   (forced_meas ? KF_FORCED_MEAS : 0) | (forced_faults ? KF_FORCED_FAULTS : 0) |
-                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0);
+                  (args->flags & CLIFFT_GPU_TRACE ? KF_TRACE : 0) |
+                  (args->flags & CLIFFT_GPU_RAW_PARITY ? KF_RAW_PARITY : 0) |
+                  (args->flags & CLIFFT_GPU_TENSOR_DENSE ? KF_DENSE : 0);
         K.rec_words = rec_words;
         K.det_words = det_words;
         K.obs_words = obs_words;
@@ -947,6 +949,10 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             Kx.state_global = Lx.state_in_smem
                                   ? nullptr
                                   : slab.get(size_t(Lx.blocks) * Lx.regions * Lx.S * Lx.state_stride * amp);
+            // dense blocks: MMA fragments of one composed matrix per CTA
+            Kx.dense_frag = ((K.flags & KF_DENSE) && args->precision == CLIFFT_GPU_FP32 && Lx.G == 0 && Lx.fuse)
+                                ? static_cast<float*>(buf.alloc(size_t(Lx.blocks) * kDenseFloats * sizeof(float)))
+                                : nullptr;
         };
         const size_t n_counters = 5 + m.num_observables;
         const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;

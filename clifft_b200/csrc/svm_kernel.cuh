@@ -125,6 +125,7 @@ struct KParams {
     uint64_t dump_shots;
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
     uint32_t stages;      // tile buffers per CTA (2..kMaxStages) when fuse_bytes != 0
+    float* dense_frag;    // KF_DENSE: per CTA kDenseFloats floats, the composed dense block's MMA fragments
     unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
     // segmented execution (survivor runs of warp groups): this launch runs
     // instructions [seg_begin, seg_end) for the items of seg_in; shots alive
@@ -145,6 +146,8 @@ enum : uint32_t {
     KF_FORCED_FAULTS = 0x04u,
     KF_TRACE = 0x10u,
     KF_FUSE = 0x20u,  // fused tile sweeps for global-memory statevectors (CTA groups)
+    KF_RAW_PARITY = 0x40u,  // detectors / observables without expected parities, POSTSELECT records instead of discarding
+    KF_DENSE = 0x80u,       // FP32 CTA groups: dense runs of a fused block on the tensor cores (3xTF32)
 };
 
 enum : uint32_t {
@@ -442,7 +445,11 @@ struct Tally {
 //     measurement first folds with an H micro-op, a fused swap with a SWAP
 //     micro-op), and the collapse to the upper half flips the shot's address
 //     label (`xo`) instead of copying it.
-enum : uint8_t { M_CNOT, M_CZ, M_SWAP, M_MCNOT, M_MCZ, M_H, M_PHASE, M_U2, M_U4, M_EXPAND, M_SCALE };
+//   * With KF_DENSE (FP32 CTA groups) a run of micro-ops that stays on at
+//     most four tile-local bits and holds an H / U2 / U4 is composed into one
+//     16 x 16 complex matrix, applied as a batched GEMM on the tensor cores
+//     (M_DENSE; the rest of the run becomes M_NOP).
+enum : uint8_t { M_CNOT, M_CZ, M_SWAP, M_MCNOT, M_MCZ, M_H, M_PHASE, M_U2, M_U4, M_EXPAND, M_SCALE, M_DENSE, M_NOP };
 enum : uint8_t {
     MF_PARITY = 0x1,  // the condition also needs odd parity of (index & par) ^ (global bits & gpar)
     MF_COPY = 0x2,    // EXPAND without a phase: a plain copy
@@ -480,6 +487,26 @@ struct TileCfg {
         return kBufOffset + stages * (1u << kBits) * 2u * (uint32_t)sizeof(R);
     }
 };
+
+// ---- tensor-core primitives of the dense blocks: TF32 rounding and the
+// m16n8k8 TF32 MMA with FP32 accumulation. A dense block's real 32 x 32
+// matrix [[Ur, -Ui], [Ui, Ur]] is stored as per-lane A fragments of its two
+// 16 x 16 halves Ur and Ui, each split into a TF32 high part and a TF32 low
+// part (x - hi); products use three MMAs (lo*hi, hi*lo, hi*hi), the split
+// that keeps the product within a few FP32 ulps.
+constexpr int kDenseFloats = 2 * 2 * 32 * 8;  // {Ur, Ui} x 2 k-halves x 32 lanes x (4 hi + 4 lo)
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
 
 // ---- bulk-copy (TMA, untiled) and mbarrier primitives. Every copy here reads
 // or writes this GPU's own global memory; none uses cluster multicast.
@@ -966,9 +993,8 @@ struct Shot {
             phase_sweep(a, zr, zi);
         }
     }
-    // Barrier of the threads that compute on tiles in a fused block: the
-    // whole group, or every warp but the copy warp of a warp-specialised CTA.
-    // threads that compute on tiles in a fused block
+    // Threads that compute on tiles in a fused block (the whole group, or
+    // every warp but the copy warp of a warp-specialised CTA) and their barrier.
     static __device__ __forceinline__ int compute_threads() {
         return Grp::kWS ? (int)blockDim.x - 32 : Grp::size();
     }
@@ -1680,13 +1706,20 @@ struct Shot {
             case CLIFFT_OP_READOUT_NOISE: readout_noise(p0); break;
             case CLIFFT_OP_DETECTOR: {
                 flush_records();
-                int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
+                int par = ((fl & CLIFFT_FLAG_EXPECTED_ONE) && !(K.flags & KF_RAW_PARITY)) ? 1 : 0;
                 par ^= list_parity(P.det_off, P.det_tg, p0);
                 if (Grp::rank() == 0 && par) det[(p1 >> 5) * S] |= 1u << (p1 & 31);
                 break;
             }
             case CLIFFT_OP_POSTSELECT: {
                 flush_records();
+                if (K.flags & KF_RAW_PARITY) {
+                    // a reference-syndrome shot: the raw parity, recorded in the
+                    // detector slot the instruction carries, no discard
+                    const int par = list_parity(P.det_off, P.det_tg, p0);
+                    if (Grp::rank() == 0 && par) det[(p1 >> 5) * S] |= 1u << (p1 & 31);
+                    break;
+                }
                 int par = (fl & CLIFFT_FLAG_EXPECTED_ONE) ? 1 : 0;
                 par ^= list_parity(P.det_off, P.det_tg, p0);
                 if (par) {
@@ -2184,6 +2217,8 @@ struct Shot {
         n_mops = 0;
         const uint32_t rend = term_kind ? term : end;
         for (uint32_t q = pc; q < rend; ++q) exec(q);
+        const int n_body = n_mops;  // the micro-ops before a terminator's own
+        (void)n_body;
         uint32_t tfa = 0, tt = 0, tidx = 0;
         int tsign = 0;
         bool red_local = false;
@@ -2201,6 +2236,25 @@ struct Shot {
             red_bit = red_local ? (uint32_t)__popcll(F & ((1ull << tt) - 1)) : tt;
         }
         resolving = false;
+        if constexpr (kDenseOk) {
+            if ((K.flags & KF_DENSE) && K.dense_frag) {
+                Grp::sync();  // the resolved micro-ops, read by every thread
+                MOp* mm = reinterpret_cast<MOp*>(fuse + fuse_mops_offset());
+                uint32_t dmask = 0;
+                int j1 = 0;
+                const int j0 = find_dense(mm, n_body, dmask, j1);
+                if (j0 >= 0) {
+                    float* frag = K.dense_frag + (size_t)blockIdx.x * kDenseFloats;
+                    if (Grp::rank() < 16) compose_dense(mm, j0, j1, dmask, Grp::rank(), frag);
+                    Grp::sync();
+                    if (Grp::rank() == 0) {
+                        mm[j0].kind = M_DENSE;
+                        mm[j0].req = dmask;
+                        for (int j = j0 + 1; j < j1; ++j) mm[j].kind = M_NOP;
+                    }
+                }
+            }
+        }
         if (Grp::rank() == 0)
             compile_index_runs(reinterpret_cast<MOp*>(fuse + fuse_mops_offset()), n_mops,
                                (1u << MB) / (uint32_t)compute_threads());
@@ -2218,6 +2272,18 @@ struct Shot {
         const int nmo = term_kind >= 2 ? nm - 1 : nm;
         auto body = [&](T* buf, uint64_t, uint64_t tbase) {
             for (int j = 0; j < nmo;) {
+                if constexpr (kDenseOk) {
+                    if (mops[j].kind == M_NOP) {
+                        ++j;
+                        continue;
+                    }
+                    if (mops[j].kind == M_DENSE) {
+                        apply_dense(mops[j].req, buf, tid, nthr, K.dense_frag + (size_t)blockIdx.x * kDenseFloats);
+                        csync();
+                        ++j;
+                        continue;
+                    }
+                }
                 int e = j;
                 while (e < nmo && index_map_kind(mops[e].kind)) ++e;
                 if (e - j >= 2 && rpt <= kMaxRunAmps) {
@@ -2575,6 +2641,252 @@ struct Shot {
         }
     }
 
+    // ---- dense blocks on the tensor cores (KF_DENSE, FP32 CTA groups)
+    static constexpr bool kDenseOk = sizeof(R) == 4 && Grp::kCta;
+    // Tile-local bits a micro-op moves or reads, or ~0u when it cannot join a
+    // dense run (an expansion, a renormalisation, a condition on tile-global
+    // bits).
+    static __device__ __forceinline__ uint32_t dense_bits(const MOp& m) {
+        if (m.greq || ((m.flags & MF_PARITY) && m.gpar)) return ~0u;
+        const uint32_t cond = m.req | ((m.flags & MF_PARITY) ? m.par : 0u);
+        switch (m.kind) {
+            case M_H:
+            case M_U2: return 1u << m.a;
+            case M_SWAP:
+            case M_U4: return (1u << m.a) | (1u << m.b);
+            case M_CNOT:
+            case M_MCNOT: return (1u << m.a) | cond;
+            case M_CZ:
+            case M_MCZ:
+            case M_PHASE: return cond;
+            default: return ~0u;
+        }
+    }
+    // Work a micro-op costs on the CUDA cores, in passes over the tile
+    static __device__ __forceinline__ int dense_weight(uint8_t kind) {
+        return kind == M_U4 ? 4 : (kind == M_U2 ? 2 : 1);
+    }
+    // The first run of micro-ops in [0, n) on at most four tile-local bits
+    // that holds a mixing op (H, U2, U4) and is worth a GEMM (weight >= 4):
+    // returns its first op (-1: none), its end in j1 and its four bits (padded
+    // with the lowest free tile bits) in dmask.
+    static __device__ int find_dense(const MOp* mops, int n, uint32_t& dmask, int& j1) {
+        constexpr uint32_t MB = TC::kBits;
+        for (int j = 0; j < n; ++j) {
+            uint32_t bits = 0;
+            bool mix = false;
+            int w = 0, e = j;
+            for (; e < n; ++e) {
+                const uint32_t b = dense_bits(mops[e]);
+                if (b == ~0u || __popc(bits | b) > 4) break;
+                bits |= b;
+                mix |= mops[e].kind == M_H || mops[e].kind == M_U2 || mops[e].kind == M_U4;
+                w += dense_weight(mops[e].kind);
+            }
+            if (e - j >= 2 && mix && w >= 4) {
+                for (uint32_t q = 0; __popc(bits) < 4 && q < MB; ++q) bits |= 1u << q;
+                dmask = bits;
+                j1 = e;
+                return j;
+            }
+        }
+        return -1;
+    }
+    // Column `col` of the 16 x 16 matrix of micro-ops [j0, j1) on the four
+    // bits of dmask (index bit q = the q-th lowest bit of dmask), composed in
+    // FP64 by applying each op to the basis vector e_col with the arithmetic
+    // of its CUDA-core handler; written as TF32 hi / lo parts of the A
+    // fragments of Ur and Ui (m16n8k8 row-major A: lane = 4 * (row % 8) +
+    // col % 4, register (row / 8) + 2 * ((col % 8) / 4), k-half col / 8).
+    static __device__ __noinline__ void compose_dense(const MOp* mops, int j0, int j1, uint32_t dmask, int col,
+                                                       float* frag) {
+        uint32_t dbit[4];
+        {
+            uint32_t w = dmask;
+            for (int q = 0; q < 4; ++q) {
+                dbit[q] = (uint32_t)__ffs(w) - 1;
+                w &= w - 1;
+            }
+        }
+        auto dm = [&](uint32_t lm) {
+            uint32_t r = 0;
+            for (int q = 0; q < 4; ++q) r |= ((lm >> dbit[q]) & 1u) << q;
+            return r;
+        };
+        double2 v[16];
+        for (int i = 0; i < 16; ++i) v[i] = make_double2(i == col ? 1.0 : 0.0, 0.0);
+        auto cd = [](const T& c) { return make_double2((double)c.x, (double)c.y); };
+        auto mul = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+        auto add = [](double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); };
+        for (int j = j0; j < j1; ++j) {
+            const MOp& m = mops[j];
+            const bool use_par = (m.flags & MF_PARITY) != 0;
+            const uint32_t req = dm(m.req), par = use_par ? dm(m.par) : 0u;
+            auto on = [&](uint32_t i) { return (i & req) == req && (!use_par || (__popc(i & par) & 1)); };
+            const uint32_t ab = dm(1u << (m.a & 31u)), bb = dm(1u << (m.b & 31u));
+            switch (m.kind) {
+                case M_CNOT:
+                case M_MCNOT:
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (!(i & ab) && on(i)) {
+                            const double2 t = v[i];
+                            v[i] = v[i | ab];
+                            v[i | ab] = t;
+                        }
+                    break;
+                case M_CZ:
+                case M_MCZ:
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (on(i)) v[i] = make_double2(-v[i].x, -v[i].y);
+                    break;
+                case M_PHASE: {
+                    const double2 ph = cd(m.c[0]);
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (on(i)) v[i] = mul(v[i], ph);
+                    break;
+                }
+                case M_SWAP:
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if ((i & ab) && !(i & bb)) {
+                            const uint32_t o = i ^ ab ^ bb;
+                            const double2 t = v[i];
+                            v[i] = v[o];
+                            v[o] = t;
+                        }
+                    break;
+                case M_H:
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (!(i & ab)) {
+                            const double2 x = v[i], y = v[i | ab];
+                            v[i] = make_double2((x.x + y.x) * CGPU_INV_SQRT2, (x.y + y.y) * CGPU_INV_SQRT2);
+                            v[i | ab] = make_double2((x.x - y.x) * CGPU_INV_SQRT2, (x.y - y.y) * CGPU_INV_SQRT2);
+                        }
+                    break;
+                case M_U2: {
+                    const double2 m00 = cd(m.c[0]), m01 = cd(m.c[1]), m10 = cd(m.c[2]), m11 = cd(m.c[3]);
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (!(i & ab)) {
+                            const double2 x = v[i], y = v[i | ab];
+                            v[i] = add(mul(m00, x), mul(m01, y));
+                            v[i | ab] = add(mul(m10, x), mul(m11, y));
+                        }
+                    break;
+                }
+                case M_U4:
+                    for (uint32_t i = 0; i < 16; ++i)
+                        if (!(i & ab) && !(i & bb)) {
+                            const double2 x[4] = {v[i], v[i | ab], v[i | bb], v[i | ab | bb]};
+                            double2 y[4];
+                            for (int r = 0; r < 4; ++r) {
+                                double2 acc = mul(cd(m.c[4 * r]), x[0]);
+                                for (int c = 1; c < 4; ++c) acc = add(acc, mul(cd(m.c[4 * r + c]), x[c]));
+                                y[r] = acc;
+                            }
+                            v[i] = y[0];
+                            v[i | ab] = y[1];
+                            v[i | bb] = y[2];
+                            v[i | ab | bb] = y[3];
+                        }
+                    break;
+                default: break;
+            }
+        }
+        const int kh = col >> 3, tig = col & 3, ch = (col >> 2) & 1;
+        for (int r = 0; r < 16; ++r) {
+            const int lane = (r & 7) * 4 + tig, idx = (r >> 3) + 2 * ch;
+            for (int which = 0; which < 2; ++which) {
+                const double x = which ? v[r].y : v[r].x;
+                const float hi = __uint_as_float(to_tf32((float)x));
+                const float lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
+                float* f = frag + ((which * 2 + kh) * 32 + lane) * 8;
+                f[idx] = hi;
+                f[4 + idx] = lo;
+            }
+        }
+    }
+    // y = U x on every 16-amplitude group of the tile (the groups vary the
+    // four bits of dmask): as real GEMMs [yr; yi] = [[Ur, -Ui], [Ui, Ur]]
+    // [xr; xi] of m16n8k8 TF32 MMAs, 8 groups per MMA column block, each
+    // product split hi / lo into three MMAs. Every warp owns whole column
+    // blocks: it reads its 8 groups into registers, multiplies, and writes
+    // them back after a warp barrier.
+    static __device__ void apply_dense(uint32_t dmask, T* tile, int tid, int nthr, const float* frag) {
+        constexpr uint32_t MB = TC::kBits;
+        constexpr uint32_t NT = (1u << (MB - 4)) / 8;  // column blocks of 8 groups
+        const uint32_t lane = (uint32_t)tid & 31u, gid = lane >> 2, tig = lane & 3u;
+        uint32_t dbit[4];
+        {
+            uint32_t w = dmask;
+            for (int q = 0; q < 4; ++q) {
+                dbit[q] = (uint32_t)__ffs(w) - 1;
+                w &= w - 1;
+            }
+        }
+        auto dpos = [&](uint32_t d) {
+            return ((d & 1u) << dbit[0]) | (((d >> 1) & 1u) << dbit[1]) | (((d >> 2) & 1u) << dbit[2]) |
+                   (((d >> 3) & 1u) << dbit[3]);
+        };
+        auto gbase = [&](uint32_t g) { return ins0_32(ins0_32(ins0_32(ins0_32(g, dbit[0]), dbit[1]), dbit[2]), dbit[3]); };
+        uint32_t ah[2][2][4], al[2][2][4];  // [Ur / Ui][k-half][register]
+#pragma unroll
+        for (int which = 0; which < 2; ++which)
+#pragma unroll
+            for (int kh = 0; kh < 2; ++kh) {
+                const float4* f = reinterpret_cast<const float4*>(frag + ((which * 2 + kh) * 32 + lane) * 8);
+                const float4 h = f[0], l = f[1];
+                ah[which][kh][0] = __float_as_uint(h.x);
+                ah[which][kh][1] = __float_as_uint(h.y);
+                ah[which][kh][2] = __float_as_uint(h.z);
+                ah[which][kh][3] = __float_as_uint(h.w);
+                al[which][kh][0] = __float_as_uint(l.x);
+                al[which][kh][1] = __float_as_uint(l.y);
+                al[which][kh][2] = __float_as_uint(l.z);
+                al[which][kh][3] = __float_as_uint(l.w);
+            }
+        const uint32_t pin[4] = {dpos(tig), dpos(tig + 4), dpos(tig + 8), dpos(tig + 12)};
+        const uint32_t q0 = dpos(gid), q1 = dpos(gid + 8);
+        for (uint32_t nt = (uint32_t)tid >> 5; nt < NT; nt += (uint32_t)nthr >> 5) {
+            const uint32_t bi = gbase(nt * 8 + gid);
+            // B fragments: k-half kh holds inputs tig + 8 kh (b0) and tig + 4 + 8 kh (b1)
+            uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const T x = tile[bi | pin[q]];
+                rh[q] = to_tf32(x.x);
+                rl[q] = to_tf32(x.x - __uint_as_float(rh[q]));
+                ih[q] = to_tf32(x.y);
+                il[q] = to_tf32(x.y - __uint_as_float(ih[q]));
+            }
+            float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
+            constexpr uint32_t NEG = 0x80000000u;
+#pragma unroll
+            for (int kh = 0; kh < 2; ++kh) {
+                const int b0 = 2 * kh, b1 = 2 * kh + 1;
+                // yr += Ur xr - Ui xi
+                mma_tf32(re, al[0][kh], rh[b0], rh[b1]);
+                mma_tf32(re, ah[0][kh], rl[b0], rl[b1]);
+                mma_tf32(re, al[1][kh], ih[b0] ^ NEG, ih[b1] ^ NEG);
+                mma_tf32(re, ah[1][kh], il[b0] ^ NEG, il[b1] ^ NEG);
+                mma_tf32(re, ah[0][kh], rh[b0], rh[b1]);
+                mma_tf32(re, ah[1][kh], ih[b0] ^ NEG, ih[b1] ^ NEG);
+                // yi += Ui xr + Ur xi
+                mma_tf32(im, al[1][kh], rh[b0], rh[b1]);
+                mma_tf32(im, ah[1][kh], rl[b0], rl[b1]);
+                mma_tf32(im, al[0][kh], ih[b0], ih[b1]);
+                mma_tf32(im, ah[0][kh], il[b0], il[b1]);
+                mma_tf32(im, ah[1][kh], rh[b0], rh[b1]);
+                mma_tf32(im, ah[0][kh], ih[b0], ih[b1]);
+            }
+            __syncwarp();
+#pragma unroll
+            for (uint32_t c = 0; c < 2; ++c) {
+                const uint32_t bo = gbase(nt * 8 + 2 * tig + c);
+                tile[bo | q0] = Cx<R>::make(re[c], im[c]);
+                tile[bo | q1] = Cx<R>::make(re[2 + c], im[2 + c]);
+            }
+        }
+    }
+
     // Whether instruction pc touches the statevector (needs every thread of a
     // CTA group) or only scalar state (frame, gamma, records, noise cursor).
     __device__ __forceinline__ bool needs_all(uint32_t pc) const {
@@ -2895,7 +3207,7 @@ struct Shot {
         const bool survived = !discarded && reachable;
         const int r = Grp::rank();
         // observables XOR expected_observables (svm.cc:236-245)
-        if (r == 0)
+        if (r == 0 && !(K.flags & KF_RAW_PARITY))
             for (uint32_t i = 0; i < P.num_obs && i < P.n_expected; ++i)
                 if (P.expected[i]) obs[(i >> 5) * S] ^= 1u << (i & 31);
         Grp::sync();

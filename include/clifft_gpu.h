@@ -72,6 +72,14 @@ extern "C" {
 #define CLIFFT_GPU_PROFILE 0x80u        /* fill phase_cycles (adds timing atomics; not for benchmarks) */
 #define CLIFFT_GPU_NO_AUTOTUNE 0x100u   /* group_threads == 0: use the built-in heuristic, no trial launches */
 #define CLIFFT_GPU_NO_SEGMENTS 0x200u   /* survivor runs: one launch, no compaction between POSTSELECT segments */
+#define CLIFFT_GPU_RAW_PARITY 0x400u   /* detectors and observables without their expected parities, POSTSELECT
+                                         recorded as a detector instead of discarding: the reference-syndrome
+                                         shot of compute_reference_syndrome (src/clifft/api/reference_syndrome.cc:9-30) */
+#define CLIFFT_GPU_TENSOR_DENSE 0x800u /* FP32, one CTA per shot, fusion on: runs of fused micro-ops on at most four
+                                         tile-local bits holding an H / U2 / U4 are composed into one 16x16 complex
+                                         matrix and applied on the tensor cores (3xTF32 MMAs). Probabilities and
+                                         amplitudes stay within FP32 tolerance but are not bit-identical to the
+                                         CUDA-core path, hence opt-in */
 
 typedef struct clifft_gpu_program clifft_gpu_program;
 

@@ -106,9 +106,19 @@ def main():
               prog.peak_rank, prog.num_instructions)
 
 
+def dense_program():
+    """A k = 20 program dense in single- and two-axis unitaries (the
+    reference's passes turn its gate runs into U2 / U4 nodes): the workload
+    of the tensor-core dense blocks, which the configured programs (CNOT, CZ,
+    SWAP and phase gates only) never form."""
+    return random_program(500, n=24, length=900, max_k=20, noise=False, classical=False, expvals=False,
+                          readout=False, expand_bias=0.2)
+
+
 def bench_programs():
     """Benchmark programs (reference bytecode passes applied) for bench.py:
-    programs/<name>.npz for configs 0, 1, 3 and the 64 programs of config 2."""
+    programs/<name>.npz for configs 0, 1, 3, the 64 programs of config 2 and
+    the dense k = 20 program."""
     outdir = os.path.join(HERE, "programs")
     os.makedirs(outdir, exist_ok=True)
     items = [("cfg0", W.lower(W.config0())),
@@ -118,6 +128,7 @@ def bench_programs():
         items.append((f"cfg2_{i:02d}", W.lower(c)))
     c4, theta = W.config4()
     items.append(("cfg4", W.lower(c4)))
+    items.append(("dense_k20", dense_program()))
     for name, raw in items:
         prog = O.ref_passes(raw, O.PASS_ALL)
         prog.name = name
