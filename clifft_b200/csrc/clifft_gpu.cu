@@ -607,6 +607,18 @@ uint64_t fnv1a(const uint8_t* p, size_t n, uint64_t h = 1469598103934665603ull) 
     return h;
 }
 
+// Least CUDA-core weight (U4 4, U2 2, any other micro-op 1) of a run that the
+// dense-block path puts on the tensor cores: CLIFFT_GPU_DENSE_MIN_WEIGHT, else
+// the default below.
+uint32_t dense_min_weight() {
+    static const uint32_t w = [] {
+        const char* e = std::getenv("CLIFFT_GPU_DENSE_MIN_WEIGHT");
+        const long v = e ? std::strtol(e, nullptr, 10) : 0;
+        return v > 0 ? (uint32_t)v : 4u;
+    }();
+    return w;
+}
+
 // Persisted tuning results: with CLIFFT_GPU_TUNE_CACHE naming a file, every
 // tuned shape is appended as "program-hash device-signature mode group" and
 // earlier lines are consulted before timing trials. The device signature is
@@ -953,6 +965,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             Kx.dense_frag = ((K.flags & KF_DENSE) && args->precision == CLIFFT_GPU_FP32 && Lx.G == 0 && Lx.fuse)
                                 ? static_cast<float*>(buf.alloc(size_t(Lx.blocks) * kDenseFloats * sizeof(float)))
                                 : nullptr;
+            Kx.dense_min_weight = dense_min_weight();
         };
         const size_t n_counters = 5 + m.num_observables;
         const bool profile = (args->flags & CLIFFT_GPU_PROFILE) != 0;

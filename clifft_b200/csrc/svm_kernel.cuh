@@ -126,6 +126,7 @@ struct KParams {
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
     uint32_t stages;      // tile buffers per CTA (2..kMaxStages) when fuse_bytes != 0
     float* dense_frag;    // KF_DENSE: per CTA kDenseFloats floats, the composed dense block's MMA fragments
+    uint32_t dense_min_weight;  // KF_DENSE: least CUDA-core weight of a run worth a GEMM (U4 4, U2 2, others 1)
     unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
     // segmented execution (survivor runs of warp groups): this launch runs
     // instructions [seg_begin, seg_end) for the items of seg_in; shots alive
@@ -489,16 +490,25 @@ struct TileCfg {
 };
 
 // ---- tensor-core primitives of the dense blocks: TF32 rounding and the
-// m16n8k8 TF32 MMA with FP32 accumulation. A dense block's real 32 x 32
-// matrix [[Ur, -Ui], [Ui, Ur]] is stored as per-lane A fragments of its two
-// 16 x 16 halves Ur and Ui, each split into a TF32 high part and a TF32 low
-// part (x - hi); products use three MMAs (lo*hi, hi*lo, hi*hi), the split
-// that keeps the product within a few FP32 ulps.
-constexpr int kDenseFloats = 2 * 2 * 32 * 8;  // {Ur, Ui} x 2 k-halves x 32 lanes x (4 hi + 4 lo)
+// m16n8k8 TF32 MMA with FP32 accumulation. A dense block U = Ur + i Ui acts
+// on x = xr + i xi by three real products (Gauss):
+//   k1 = (Ur + Ui) xr,  k2 = Ur (xi - xr),  k3 = Ui (xr + xi),
+//   Re(U x) = k1 - k3,  Im(U x) = k1 + k2,
+// each operand split into a TF32 high part and the TF32 low part of the
+// remainder, each product three MMAs (lo*hi, hi*lo, hi*hi): the split that
+// keeps a product within a few FP32 ulps. The three 16 x 16 matrices are
+// stored as per-lane A fragments.
+constexpr int kDenseFloats = 3 * 2 * 32 * 8;  // {Ur + Ui, Ur, Ui} x 2 k-halves x 32 lanes x (4 hi + 4 lo)
 __device__ __forceinline__ uint32_t to_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
     return r;
+}
+// x = hi + lo exactly (hi: x with its 13 low mantissa bits cleared); lo
+// keeps its TF32 part
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+    hi = __float_as_uint(x) & 0xffffe000u;
+    lo = __float_as_uint(x - __uint_as_float(hi)) & 0xffffe000u;
 }
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -2242,7 +2252,7 @@ struct Shot {
                 MOp* mm = reinterpret_cast<MOp*>(fuse + fuse_mops_offset());
                 uint32_t dmask = 0;
                 int j1 = 0;
-                const int j0 = find_dense(mm, n_body, dmask, j1);
+                const int j0 = find_dense(mm, n_body, (int)K.dense_min_weight, dmask, j1);
                 if (j0 >= 0) {
                     float* frag = K.dense_frag + (size_t)blockIdx.x * kDenseFloats;
                     if (Grp::rank() < 16) compose_dense(mm, j0, j1, dmask, Grp::rank(), frag);
@@ -2667,10 +2677,10 @@ struct Shot {
         return kind == M_U4 ? 4 : (kind == M_U2 ? 2 : 1);
     }
     // The first run of micro-ops in [0, n) on at most four tile-local bits
-    // that holds a mixing op (H, U2, U4) and is worth a GEMM (weight >= 4):
-    // returns its first op (-1: none), its end in j1 and its four bits (padded
-    // with the lowest free tile bits) in dmask.
-    static __device__ int find_dense(const MOp* mops, int n, uint32_t& dmask, int& j1) {
+    // that holds a mixing op (H, U2, U4) and is worth a GEMM (weight >=
+    // min_weight): returns its first op (-1: none), its end in j1 and its
+    // four bits (padded with the lowest free tile bits) in dmask.
+    static __device__ int find_dense(const MOp* mops, int n, int min_weight, uint32_t& dmask, int& j1) {
         constexpr uint32_t MB = TC::kBits;
         for (int j = 0; j < n; ++j) {
             uint32_t bits = 0;
@@ -2683,7 +2693,7 @@ struct Shot {
                 mix |= mops[e].kind == M_H || mops[e].kind == M_U2 || mops[e].kind == M_U4;
                 w += dense_weight(mops[e].kind);
             }
-            if (e - j >= 2 && mix && w >= 4) {
+            if (e - j >= 2 && mix && w >= min_weight) {
                 for (uint32_t q = 0; __popc(bits) < 4 && q < MB; ++q) bits |= 1u << q;
                 dmask = bits;
                 j1 = e;
@@ -2696,8 +2706,8 @@ struct Shot {
     // bits of dmask (index bit q = the q-th lowest bit of dmask), composed in
     // FP64 by applying each op to the basis vector e_col with the arithmetic
     // of its CUDA-core handler; written as TF32 hi / lo parts of the A
-    // fragments of Ur and Ui (m16n8k8 row-major A: lane = 4 * (row % 8) +
-    // col % 4, register (row / 8) + 2 * ((col % 8) / 4), k-half col / 8).
+    // fragments of Ur + Ui, Ur and Ui (m16n8k8 row-major A: lane = 4 * (row %
+    // 8) + col % 4, register (row / 8) + 2 * ((col % 8) / 4), k-half col / 8).
     static __device__ __noinline__ void compose_dense(const MOp* mops, int j0, int j1, uint32_t dmask, int col,
                                                        float* frag) {
         uint32_t dbit[4];
@@ -2794,8 +2804,8 @@ struct Shot {
         const int kh = col >> 3, tig = col & 3, ch = (col >> 2) & 1;
         for (int r = 0; r < 16; ++r) {
             const int lane = (r & 7) * 4 + tig, idx = (r >> 3) + 2 * ch;
-            for (int which = 0; which < 2; ++which) {
-                const double x = which ? v[r].y : v[r].x;
+            for (int which = 0; which < 3; ++which) {
+                const double x = which == 0 ? v[r].x + v[r].y : (which == 1 ? v[r].x : v[r].y);
                 const float hi = __uint_as_float(to_tf32((float)x));
                 const float lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
                 float* f = frag + ((which * 2 + kh) * 32 + lane) * 8;
@@ -2805,11 +2815,10 @@ struct Shot {
         }
     }
     // y = U x on every 16-amplitude group of the tile (the groups vary the
-    // four bits of dmask): as real GEMMs [yr; yi] = [[Ur, -Ui], [Ui, Ur]]
-    // [xr; xi] of m16n8k8 TF32 MMAs, 8 groups per MMA column block, each
-    // product split hi / lo into three MMAs. Every warp owns whole column
-    // blocks: it reads its 8 groups into registers, multiplies, and writes
-    // them back after a warp barrier.
+    // four bits of dmask) as three real 16 x 16 GEMMs (Gauss form above) of
+    // m16n8k8 TF32 MMAs, 8 groups per MMA column block. Every warp owns
+    // whole column blocks: it reads its 8 groups into registers, multiplies,
+    // and writes them back after a warp barrier.
     static __device__ void apply_dense(uint32_t dmask, T* tile, int tid, int nthr, const float* frag) {
         constexpr uint32_t MB = TC::kBits;
         constexpr uint32_t NT = (1u << (MB - 4)) / 8;  // column blocks of 8 groups
@@ -2827,9 +2836,9 @@ struct Shot {
                    (((d >> 3) & 1u) << dbit[3]);
         };
         auto gbase = [&](uint32_t g) { return ins0_32(ins0_32(ins0_32(ins0_32(g, dbit[0]), dbit[1]), dbit[2]), dbit[3]); };
-        uint32_t ah[2][2][4], al[2][2][4];  // [Ur / Ui][k-half][register]
+        uint32_t ah[3][2][4], al[3][2][4];  // [Ur + Ui / Ur / Ui][k-half][register]
 #pragma unroll
-        for (int which = 0; which < 2; ++which)
+        for (int which = 0; which < 3; ++which)
 #pragma unroll
             for (int kh = 0; kh < 2; ++kh) {
                 const float4* f = reinterpret_cast<const float4*>(frag + ((which * 2 + kh) * 32 + lane) * 8);
@@ -2848,41 +2857,34 @@ struct Shot {
         for (uint32_t nt = (uint32_t)tid >> 5; nt < NT; nt += (uint32_t)nthr >> 5) {
             const uint32_t bi = gbase(nt * 8 + gid);
             // B fragments: k-half kh holds inputs tig + 8 kh (b0) and tig + 4 + 8 kh (b1)
-            uint32_t rh[4], rl[4], ih[4], il[4];
+            uint32_t rh[4], rl[4], dh[4], dl[4], sh[4], sl[4];  // xr, xi - xr, xr + xi
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const T x = tile[bi | pin[q]];
-                rh[q] = to_tf32(x.x);
-                rl[q] = to_tf32(x.x - __uint_as_float(rh[q]));
-                ih[q] = to_tf32(x.y);
-                il[q] = to_tf32(x.y - __uint_as_float(ih[q]));
+                split_tf32(x.x, rh[q], rl[q]);
+                split_tf32(x.y - x.x, dh[q], dl[q]);
+                split_tf32(x.x + x.y, sh[q], sl[q]);
             }
-            float re[4] = {0.f, 0.f, 0.f, 0.f}, im[4] = {0.f, 0.f, 0.f, 0.f};
-            constexpr uint32_t NEG = 0x80000000u;
+            float k1[4] = {0.f, 0.f, 0.f, 0.f}, k2[4] = {0.f, 0.f, 0.f, 0.f}, k3[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
             for (int kh = 0; kh < 2; ++kh) {
                 const int b0 = 2 * kh, b1 = 2 * kh + 1;
-                // yr += Ur xr - Ui xi
-                mma_tf32(re, al[0][kh], rh[b0], rh[b1]);
-                mma_tf32(re, ah[0][kh], rl[b0], rl[b1]);
-                mma_tf32(re, al[1][kh], ih[b0] ^ NEG, ih[b1] ^ NEG);
-                mma_tf32(re, ah[1][kh], il[b0] ^ NEG, il[b1] ^ NEG);
-                mma_tf32(re, ah[0][kh], rh[b0], rh[b1]);
-                mma_tf32(re, ah[1][kh], ih[b0] ^ NEG, ih[b1] ^ NEG);
-                // yi += Ui xr + Ur xi
-                mma_tf32(im, al[1][kh], rh[b0], rh[b1]);
-                mma_tf32(im, ah[1][kh], rl[b0], rl[b1]);
-                mma_tf32(im, al[0][kh], ih[b0], ih[b1]);
-                mma_tf32(im, ah[0][kh], il[b0], il[b1]);
-                mma_tf32(im, ah[1][kh], rh[b0], rh[b1]);
-                mma_tf32(im, ah[0][kh], ih[b0], ih[b1]);
+                mma_tf32(k1, al[0][kh], rh[b0], rh[b1]);
+                mma_tf32(k1, ah[0][kh], rl[b0], rl[b1]);
+                mma_tf32(k2, al[1][kh], dh[b0], dh[b1]);
+                mma_tf32(k2, ah[1][kh], dl[b0], dl[b1]);
+                mma_tf32(k3, al[2][kh], sh[b0], sh[b1]);
+                mma_tf32(k3, ah[2][kh], sl[b0], sl[b1]);
+                mma_tf32(k1, ah[0][kh], rh[b0], rh[b1]);
+                mma_tf32(k2, ah[1][kh], dh[b0], dh[b1]);
+                mma_tf32(k3, ah[2][kh], sh[b0], sh[b1]);
             }
             __syncwarp();
 #pragma unroll
             for (uint32_t c = 0; c < 2; ++c) {
                 const uint32_t bo = gbase(nt * 8 + 2 * tig + c);
-                tile[bo | q0] = Cx<R>::make(re[c], im[c]);
-                tile[bo | q1] = Cx<R>::make(re[2 + c], im[2 + c]);
+                tile[bo | q0] = make_float2(k1[c] - k3[c], k1[c] + k2[c]);
+                tile[bo | q1] = make_float2(k1[2 + c] - k3[2 + c], k1[2 + c] + k2[2 + c]);
             }
         }
     }
