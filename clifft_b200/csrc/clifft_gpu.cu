@@ -260,7 +260,7 @@ struct clifft_gpu_program {
                                       // probability (clifft::noise_site_probabilities order)
     // launch shapes already planned for this program (see plan_launch)
     mutable std::mutex plan_mu;
-    mutable std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t, uint32_t, uint32_t>, std::vector<uint8_t>>
+    mutable std::map<std::tuple<uint32_t, uint32_t, bool, uint32_t, uint32_t, uint32_t, bool>, std::vector<uint8_t>>
         plan_cache;
     // Statevector slab kept between calls (mapping tens of GB afresh on every
     // call costs more than a large-k launch's own setup). One call at a time
@@ -353,9 +353,11 @@ constexpr uint32_t kWsThreads = 544, kWsThreadsHalf = 288;
 bool ws_shape(uint32_t threads) { return threads == kWsThreads || threads == kWsThreadsHalf; }
 
 // Shared-memory scratch of the tile engine for one shot group.
-uint32_t tile_scratch_bytes(uint32_t precision, bool cta, uint32_t stages) {
+// dense: with the B operand of the tensor-core dense blocks (FP32 CTA groups
+// with three stages only)
+uint32_t tile_scratch_bytes(uint32_t precision, bool cta, uint32_t stages, bool dense = false) {
     if (precision == CLIFFT_GPU_FP32)
-        return cta ? TileCfg<float, true>::smem_bytes(stages) : TileCfg<float, false>::smem_bytes(stages);
+        return cta ? TileCfg<float, true>::smem_bytes(stages, dense) : TileCfg<float, false>::smem_bytes(stages);
     return cta ? TileCfg<double, true>::smem_bytes(stages) : TileCfg<double, false>::smem_bytes(stages);
 }
 
@@ -378,7 +380,7 @@ struct PlanShape {
 };
 
 PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req, uint32_t rec_words,
-                     uint32_t det_words, uint32_t obs_words, bool allow_fusion) {
+                     uint32_t det_words, uint32_t obs_words, bool allow_fusion, bool dense) {
     LaunchPlan L{};
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const uint64_t stride = uint64_t(1) << p.meta.peak_rank;
@@ -419,7 +421,8 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
     L.stages = G == 32 ? 2 : 0;
     auto region_bytes = [&](bool in_smem) {
         size_t fuse = 0;  // tile-engine scratch of the group
-        if ((G == 0 || G == 32) && !in_smem) fuse = tile_scratch_bytes(precision, G == 0, L.stages);
+        if ((G == 0 || G == 32) && !in_smem)
+            fuse = tile_scratch_bytes(precision, G == 0, L.stages, dense && allow_fusion);
         return ((in_smem ? state_bytes * L.S : 0) + ((rec_bytes1 * L.S + 15) & ~size_t(15)) + fuse + 15) &
                ~size_t(15);
     };
@@ -517,8 +520,8 @@ void keep_pool_memory(int dev) {
 // the device queries; the grid is sized per call.
 LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t group_req,
                        uint64_t shots, uint32_t rec_words, uint32_t det_words, uint32_t obs_words,
-                       bool allow_fusion, uint32_t max_resident = 0) {
-    const auto key = std::make_tuple(precision, group_req, allow_fusion, rec_words, det_words, obs_words);
+                       bool allow_fusion, uint32_t max_resident = 0, bool dense = false) {
+    const auto key = std::make_tuple(precision, group_req, allow_fusion, rec_words, det_words, obs_words, dense);
     PlanShape ps;
     {
         std::lock_guard<std::mutex> lock(p.plan_mu);
@@ -526,7 +529,7 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         if (it != p.plan_cache.end()) {
             std::memcpy(&ps, it->second.data(), sizeof(PlanShape));
         } else {
-            ps = plan_shape(p, precision, group_req, rec_words, det_words, obs_words, allow_fusion);
+            ps = plan_shape(p, precision, group_req, rec_words, det_words, obs_words, allow_fusion, dense);
             std::vector<uint8_t> blob(sizeof(PlanShape));
             std::memcpy(blob.data(), &ps, sizeof(PlanShape));
             p.plan_cache.emplace(key, std::move(blob));
@@ -932,8 +935,9 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
                 tune = tune_candidates(*prog, args->precision);
             }
         }
+        const bool want_dense = (args->flags & CLIFFT_GPU_TENSOR_DENSE) && args->precision == CLIFFT_GPU_FP32;
         LaunchPlan L = plan_launch(*prog, args->precision, group_req, shots, rec_words, det_words, obs_words,
-                                   allow_fusion, args->max_resident);
+                                   allow_fusion, args->max_resident, want_dense);
         KParams K{};
         K.shots = shots;
         K.first_shot = args->first_shot;
@@ -954,17 +958,18 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
         // launch-shape dependent parameters (and the statevector slab)
         auto apply_plan = [&](KParams& Kx, const LaunchPlan& Lx) {
             Kx.flags = (K.flags & ~uint32_t(KF_FUSE)) | (Lx.fuse ? KF_FUSE : 0);
-            Kx.fuse_bytes = Lx.tiles ? tile_scratch_bytes(args->precision, Lx.G == 0, Lx.stages) : 0;
+            // dense blocks on the tensor cores: FP32 CTA groups of 256 compute
+            // threads (three tile stages) streaming fused blocks; other shapes
+            // run the same blocks on the CUDA cores
+            const bool dense_ok = want_dense && Lx.G == 0 && Lx.fuse && Lx.stages == 3;
+            if (!dense_ok) Kx.flags &= ~uint32_t(KF_DENSE);
+            Kx.fuse_bytes = Lx.tiles ? tile_scratch_bytes(args->precision, Lx.G == 0, Lx.stages, dense_ok) : 0;
             Kx.stages = Lx.stages;
             Kx.state_in_smem = Lx.state_in_smem ? 1 : 0;
             Kx.state_stride = Lx.state_stride;
             Kx.state_global = Lx.state_in_smem
                                   ? nullptr
                                   : slab.get(size_t(Lx.blocks) * Lx.regions * Lx.S * Lx.state_stride * amp);
-            // dense blocks: MMA fragments of one composed matrix per CTA
-            Kx.dense_frag = ((K.flags & KF_DENSE) && args->precision == CLIFFT_GPU_FP32 && Lx.G == 0 && Lx.fuse)
-                                ? static_cast<float*>(buf.alloc(size_t(Lx.blocks) * kDenseFloats * sizeof(float)))
-                                : nullptr;
             Kx.dense_min_weight = dense_min_weight();
         };
         const size_t n_counters = 5 + m.num_observables;
@@ -1056,7 +1061,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             uint32_t best = 0;
             for (uint32_t cand : tune) {
                 LaunchPlan Lc = plan_launch(*prog, args->precision, cand, shots, rec_words, det_words, obs_words,
-                                            allow_fusion, args->max_resident);
+                                            allow_fusion, args->max_resident, want_dense);
                 const uint64_t wave = uint64_t(Lc.blocks) * Lc.regions * Lc.S;
                 const uint64_t trial = std::min<uint64_t>(shots, 2 * wave);
                 KParams Kc = K;
@@ -1089,7 +1094,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
                 tune_file_store(prog->content_hash, prog->device, tune_key, best);
             }
             L = plan_launch(*prog, args->precision, best, shots, rec_words, det_words, obs_words, allow_fusion,
-                            args->max_resident);
+                            args->max_resident, want_dense);
         }
         apply_plan(K, L);
         // Survivor runs of warp groups go segment by segment: the program is cut

@@ -125,7 +125,6 @@ struct KParams {
     uint64_t dump_shots;
     uint32_t fuse_bytes;  // shared bytes per CTA reserved for fused tile sweeps (0 = off)
     uint32_t stages;      // tile buffers per CTA (2..kMaxStages) when fuse_bytes != 0
-    float* dense_frag;    // KF_DENSE: per CTA kDenseFloats floats, the composed dense block's MMA fragments
     uint32_t dense_min_weight;  // KF_DENSE: least CUDA-core weight of a run worth a GEMM (U4 4, U2 2, others 1)
     unsigned long long* phase_cycles;  // optional: SM cycles per executor phase (thread 0 of each group)
     // segmented execution (survivor runs of warp groups): this launch runs
@@ -148,7 +147,7 @@ enum : uint32_t {
     KF_TRACE = 0x10u,
     KF_FUSE = 0x20u,  // fused tile sweeps for global-memory statevectors (CTA groups)
     KF_RAW_PARITY = 0x40u,  // detectors / observables without expected parities, POSTSELECT records instead of discarding
-    KF_DENSE = 0x80u,       // FP32 CTA groups: dense runs of a fused block on the tensor cores (3xTF32)
+    KF_DENSE = 0x80u,       // FP32 CTA groups of 256 compute threads: dense runs of fused blocks on tcgen05 (3xTF32)
 };
 
 enum : uint32_t {
@@ -472,33 +471,42 @@ constexpr int kMaxRunsLog2 = 6;    // at most 64 contiguous runs per tile
 // tiles through two buffers and fuses up to 24 (FP32) / 16 (FP64), which
 // leaves room for four 4-warp CTAs per SM (the register limit). Scratch
 // layout of one group: [2 x kMaxStages mbarriers: tile loaded / tile computed]
-// [micro-ops][64 run offsets][64-byte axis -> local bit table]
-// [stages tile buffers, 128-B aligned].
+// [dense-block slot: MMA mbarrier, TMEM address, phase][micro-ops][64 run
+// offsets][64-byte axis -> local bit table][stages tile buffers, 128-B
+// aligned][FP32 CTA groups with three stages: the dense block's B operand,
+// 8 KiB].
 template <typename R, bool CTA>
 struct TileCfg {
     using MOp = MicroOpT<typename Cx<R>::T>;
     static constexpr int kBits = CTA ? (sizeof(R) == 4 ? 12 : 11) : (sizeof(R) == 4 ? 9 : 8);
     static constexpr int kMops = CTA ? 24 : (sizeof(R) == 4 ? 24 : 16);
     static constexpr uint32_t kBarOffset = 0;
-    static constexpr uint32_t kMopsOffset = 2u * kMaxStages * 8u;
+    static constexpr uint32_t kDenseSlotOffset = 2u * kMaxStages * 8u;
+    static constexpr uint32_t kMopsOffset = kDenseSlotOffset + 16u;
     static constexpr uint32_t kTablesOffset = kMopsOffset + kMops * (uint32_t)sizeof(MOp);
     static constexpr uint32_t kLbitOffset = kTablesOffset + 64u * 8u;
     static constexpr uint32_t kBufOffset = (kLbitOffset + 64u + 127u) & ~127u;
-    static __host__ __device__ constexpr uint32_t smem_bytes(uint32_t stages) {
+    static constexpr uint32_t kDenseBBytes = 8192u;  // B operand of a dense block: TF32 hi + lo, 32 x 32 each
+    static __host__ __device__ constexpr bool dense_capable(uint32_t stages) {
+        return CTA && sizeof(R) == 4 && stages == 3;
+    }
+    static __host__ __device__ constexpr uint32_t dense_b_offset(uint32_t stages) {
         return kBufOffset + stages * (1u << kBits) * 2u * (uint32_t)sizeof(R);
+    }
+    static __host__ __device__ constexpr uint32_t smem_bytes(uint32_t stages, bool dense = false) {
+        return dense_b_offset(stages) + (dense && dense_capable(stages) ? kDenseBBytes : 0u);
     }
 };
 
-// ---- tensor-core primitives of the dense blocks: TF32 rounding and the
-// m16n8k8 TF32 MMA with FP32 accumulation. A dense block U = Ur + i Ui acts
-// on x = xr + i xi by three real products (Gauss):
-//   k1 = (Ur + Ui) xr,  k2 = Ur (xi - xr),  k3 = Ui (xr + xi),
-//   Re(U x) = k1 - k3,  Im(U x) = k1 + k2,
-// each operand split into a TF32 high part and the TF32 low part of the
-// remainder, each product three MMAs (lo*hi, hi*lo, hi*hi): the split that
-// keeps a product within a few FP32 ulps. The three 16 x 16 matrices are
-// stored as per-lane A fragments.
-constexpr int kDenseFloats = 3 * 2 * 32 * 8;  // {Ur + Ui, Ur, Ui} x 2 k-halves x 32 lanes x (4 hi + 4 lo)
+// ---- tensor-core primitives of the dense blocks (tcgen05, TMEM). A dense
+// block U = Ur + i Ui acts on every 16-amplitude group x of a tile as one
+// real product y = M x with the 32 x 32 matrix M = [[Ur, -Ui], [Ui, Ur]] in
+// the interleaved order (index 2 d + 0 = Re, 2 d + 1 = Im): D = X M^T with
+// the groups as the 128 rows of X (one TMEM lane each, the A operand), M^T
+// as the K-major B operand in shared memory and D in TMEM. Both operands
+// are split into a TF32 high part and the TF32 low part of the remainder;
+// D = Xhi Mhi + Xlo Mhi + Xhi Mlo (3xTF32) keeps a product within a few
+// FP32 ulps. One thread issues the MMAs; the group's threads read D back.
 __device__ __forceinline__ uint32_t to_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -510,14 +518,56 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
     hi = __float_as_uint(x) & 0xffffe000u;
     lo = __float_as_uint(x - __uint_as_float(hi)) & 0xffffe000u;
 }
-__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+constexpr uint32_t kDenseTmemCols = 256;  // two 128-group chunks x (A hi 32 + A lo 32 + D 32) columns
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12
+// = 2), both K-major, N = 32 (bits 17-22 = N / 8), M = 128 (bits 24-28 = M / 16)
+constexpr uint32_t kDenseIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// shared-memory descriptor of a K-major operand without swizzle: 8-row x
+// 16-byte core matrices, LBO = 512 B between the two core matrices of an
+// MMA's K = 8, SBO = 128 B between 8-row groups, version 1 (bits 46-47)
+__device__ __forceinline__ uint64_t dense_b_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3fffu) | ((uint64_t)(512u >> 4) << 16) | ((uint64_t)(128u >> 4) << 32) |
+           (1ull << 46);
 }
-
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_alloc(uint32_t smem_dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_dst), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+// D (+)= A B with A in TMEM, B by descriptor; accumulate = 0 overwrites D
+__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t accumulate) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %3, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %4, {%5, %5, %5, %5}, p;\n}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b_desc), "r"(accumulate), "r"(kDenseIdesc), "r"(z)
+        : "memory");
+}
 // ---- bulk-copy (TMA, untiled) and mbarrier primitives. Every copy here reads
 // or writes this GPU's own global memory; none uses cluster multicast.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -554,6 +604,11 @@ __device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.
 __device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// the mbarrier completes once every tcgen05.mma this thread issued has finished
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_u32(bar))
+                 : "memory");
+}
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -2247,15 +2302,17 @@ struct Shot {
         }
         resolving = false;
         if constexpr (kDenseOk) {
-            if ((K.flags & KF_DENSE) && K.dense_frag) {
+            if (K.flags & KF_DENSE) {
                 Grp::sync();  // the resolved micro-ops, read by every thread
                 MOp* mm = reinterpret_cast<MOp*>(fuse + fuse_mops_offset());
                 uint32_t dmask = 0;
                 int j1 = 0;
-                const int j0 = find_dense(mm, n_body, (int)K.dense_min_weight, dmask, j1);
+                const int j0 = find_dense(mm, n_body, (int)K.dense_min_weight, local_mask(fresh), dmask, j1);
                 if (j0 >= 0) {
-                    float* frag = K.dense_frag + (size_t)blockIdx.x * kDenseFloats;
-                    if (Grp::rank() < 16) compose_dense(mm, j0, j1, dmask, Grp::rank(), frag);
+                    if (Grp::rank() < 16)
+                        compose_dense(mm, j0, j1, dmask, Grp::rank(),
+                                      reinterpret_cast<float*>(fuse + TC::dense_b_offset(K.stages)));
+                    fence_async_shared();  // the B operand, read by the tensor cores
                     Grp::sync();
                     if (Grp::rank() == 0) {
                         mm[j0].kind = M_DENSE;
@@ -2288,7 +2345,7 @@ struct Shot {
                         continue;
                     }
                     if (mops[j].kind == M_DENSE) {
-                        apply_dense(mops[j].req, buf, tid, nthr, K.dense_frag + (size_t)blockIdx.x * kDenseFloats);
+                        apply_dense(mops[j].req, buf, tid);
                         csync();
                         ++j;
                         continue;
@@ -2676,12 +2733,20 @@ struct Shot {
     static __device__ __forceinline__ int dense_weight(uint8_t kind) {
         return kind == M_U4 ? 4 : (kind == M_U2 ? 2 : 1);
     }
-    // The first run of micro-ops in [0, n) on at most four tile-local bits
+    // The heaviest run of micro-ops in [0, n) on at most four tile-local bits
     // that holds a mixing op (H, U2, U4) and is worth a GEMM (weight >=
-    // min_weight): returns its first op (-1: none), its end in j1 and its
-    // four bits (padded with the lowest free tile bits) in dmask.
-    static __device__ int find_dense(const MOp* mops, int n, int min_weight, uint32_t& dmask, int& j1) {
+    // min_weight; the first of equal weights): returns its first op (-1:
+    // none), its end in j1 and its
+    // four bits in dmask, padded with the highest free tile bits outside
+    // `avoid`. The bits of axes the block creates are avoided: until their
+    // EXPAND their set half of the tile is not loaded, and a GEMM would
+    // multiply that memory (possibly NaN / Inf) by the zero coefficients of
+    // the identity on a padding bit.
+    static __device__ int find_dense(const MOp* mops, int n, int min_weight, uint32_t avoid, uint32_t& dmask,
+                                     int& j1) {
         constexpr uint32_t MB = TC::kBits;
+        int best = -1, best_w = min_weight - 1;
+        uint32_t best_bits = 0;
         for (int j = 0; j < n; ++j) {
             uint32_t bits = 0;
             bool mix = false;
@@ -2693,23 +2758,31 @@ struct Shot {
                 mix |= mops[e].kind == M_H || mops[e].kind == M_U2 || mops[e].kind == M_U4;
                 w += dense_weight(mops[e].kind);
             }
-            if (e - j >= 2 && mix && w >= min_weight) {
-                for (uint32_t q = 0; __popc(bits) < 4 && q < MB; ++q) bits |= 1u << q;
-                dmask = bits;
+            if (e - j >= 2 && mix && w > best_w) {
+                best = j;
+                best_w = w;
+                best_bits = bits;
                 j1 = e;
-                return j;
             }
         }
-        return -1;
+        if (best >= 0) {
+            // padding from the top: groups then vary in the low tile bits,
+            // which spreads a warp's accesses over the shared-memory banks
+            for (int q = (int)MB - 1; __popc(best_bits) < 4 && q >= 0; --q)
+                if (!((avoid >> q) & 1u)) best_bits |= 1u << q;
+            dmask = best_bits;
+        }
+        return best;
     }
-    // Column `col` of the 16 x 16 matrix of micro-ops [j0, j1) on the four
+    // Column `col` of the 16 x 16 matrix U of micro-ops [j0, j1) on the four
     // bits of dmask (index bit q = the q-th lowest bit of dmask), composed in
     // FP64 by applying each op to the basis vector e_col with the arithmetic
-    // of its CUDA-core handler; written as TF32 hi / lo parts of the A
-    // fragments of Ur + Ui, Ur and Ui (m16n8k8 row-major A: lane = 4 * (row %
-    // 8) + col % 4, register (row / 8) + 2 * ((col % 8) / 4), k-half col / 8).
+    // of its CUDA-core handler; written as its entries of M (rows n = 2 d + c
+    // of the outputs, columns k = 2 col + c' of the inputs) into the K-major
+    // B operand: element (n, k) at byte (k / 4) * 512 + (n / 8) * 128 +
+    // (n % 8) * 16 + (k % 4) * 4, TF32 high parts first, low parts 4 KiB on.
     static __device__ __noinline__ void compose_dense(const MOp* mops, int j0, int j1, uint32_t dmask, int col,
-                                                       float* frag) {
+                                                       float* bop) {
         uint32_t dbit[4];
         {
             uint32_t w = dmask;
@@ -2801,92 +2874,109 @@ struct Shot {
                 default: break;
             }
         }
-        const int kh = col >> 3, tig = col & 3, ch = (col >> 2) & 1;
-        for (int r = 0; r < 16; ++r) {
-            const int lane = (r & 7) * 4 + tig, idx = (r >> 3) + 2 * ch;
-            for (int which = 0; which < 3; ++which) {
-                const double x = which == 0 ? v[r].x + v[r].y : (which == 1 ? v[r].x : v[r].y);
+        // M[2d][2col] = Re U[d][col], M[2d+1][2col] = Im, M[2d][2col+1] = -Im, M[2d+1][2col+1] = Re
+        for (int d = 0; d < 16; ++d)
+            for (int c = 0; c < 4; ++c) {
+                const int n = 2 * d + (c & 1), k = 2 * col + (c >> 1);
+                const double x = c == 0 ? v[d].x : (c == 1 ? v[d].y : (c == 2 ? -v[d].y : v[d].x));
                 const float hi = __uint_as_float(to_tf32((float)x));
                 const float lo = __uint_as_float(to_tf32((float)(x - (double)hi)));
-                float* f = frag + ((which * 2 + kh) * 32 + lane) * 8;
-                f[idx] = hi;
-                f[4 + idx] = lo;
+                const int off = (k >> 2) * 128 + (n >> 3) * 32 + (n & 7) * 4 + (k & 3);  // in floats
+                bop[off] = hi;
+                bop[1024 + off] = lo;
             }
-        }
     }
     // y = U x on every 16-amplitude group of the tile (the groups vary the
-    // four bits of dmask) as three real 16 x 16 GEMMs (Gauss form above) of
-    // m16n8k8 TF32 MMAs, 8 groups per MMA column block. Every warp owns
-    // whole column blocks: it reads its 8 groups into registers, multiplies,
-    // and writes them back after a warp barrier.
-    static __device__ void apply_dense(uint32_t dmask, T* tile, int tid, int nthr, const float* frag) {
-        constexpr uint32_t MB = TC::kBits;
-        constexpr uint32_t NT = (1u << (MB - 4)) / 8;  // column blocks of 8 groups
-        const uint32_t lane = (uint32_t)tid & 31u, gid = lane >> 2, tig = lane & 3u;
+    // four bits of dmask) on the tensor cores. The 256 groups form two
+    // 128-row chunks; compute warp w writes rows 32 (w % 4) .. + 31 of chunk
+    // w / 4 (its TMEM lane quarter) as TF32 hi / lo columns, thread 0 issues
+    // the 24 MMAs (per chunk: 4 K-steps x 3 products) and commits them to the
+    // dense mbarrier, every thread waits for it (bounded), reads its row of
+    // D and writes its group back. The waits of all compute threads agree;
+    // a wait that gives up records a device error and turns the dense path
+    // off for the rest of the launch on this CTA.
+    __device__ void apply_dense(uint32_t dmask, T* tile, int tid) {
+        uint32_t* slot = reinterpret_cast<uint32_t*>(fuse + TC::kDenseSlotOffset);
+        uint64_t* bar = reinterpret_cast<uint64_t*>(slot);
+        const uint32_t state = slot[3];  // bit 0: the mbarrier's phase, bit 31: off after a timeout
+        if (state >> 31) return;
+        const uint32_t tmem = slot[2];
+        const uint32_t w = (uint32_t)tid >> 5, lane = (uint32_t)tid & 31u, ch = w >> 2, qr = w & 3u;
         uint32_t dbit[4];
         {
-            uint32_t w = dmask;
+            uint32_t m = dmask;
             for (int q = 0; q < 4; ++q) {
-                dbit[q] = (uint32_t)__ffs(w) - 1;
-                w &= w - 1;
+                dbit[q] = (uint32_t)__ffs(m) - 1;
+                m &= m - 1;
             }
         }
         auto dpos = [&](uint32_t d) {
             return ((d & 1u) << dbit[0]) | (((d >> 1) & 1u) << dbit[1]) | (((d >> 2) & 1u) << dbit[2]) |
                    (((d >> 3) & 1u) << dbit[3]);
         };
-        auto gbase = [&](uint32_t g) { return ins0_32(ins0_32(ins0_32(ins0_32(g, dbit[0]), dbit[1]), dbit[2]), dbit[3]); };
-        uint32_t ah[3][2][4], al[3][2][4];  // [Ur + Ui / Ur / Ui][k-half][register]
+        const uint32_t g = (ch << 7) | (qr << 5) | lane;
+        const uint32_t base = ins0_32(ins0_32(ins0_32(ins0_32(g, dbit[0]), dbit[1]), dbit[2]), dbit[3]);
+        const uint32_t cols = tmem + ((qr * 32u) << 16) + ch * 96u;  // this warp's lanes, the chunk's columns
+        tc_fence_after();
 #pragma unroll
-        for (int which = 0; which < 3; ++which)
+        for (uint32_t p = 0; p < 4; ++p) {
+            uint32_t hi[8], lo[8];
 #pragma unroll
-            for (int kh = 0; kh < 2; ++kh) {
-                const float4* f = reinterpret_cast<const float4*>(frag + ((which * 2 + kh) * 32 + lane) * 8);
-                const float4 h = f[0], l = f[1];
-                ah[which][kh][0] = __float_as_uint(h.x);
-                ah[which][kh][1] = __float_as_uint(h.y);
-                ah[which][kh][2] = __float_as_uint(h.z);
-                ah[which][kh][3] = __float_as_uint(h.w);
-                al[which][kh][0] = __float_as_uint(l.x);
-                al[which][kh][1] = __float_as_uint(l.y);
-                al[which][kh][2] = __float_as_uint(l.z);
-                al[which][kh][3] = __float_as_uint(l.w);
+            for (uint32_t e = 0; e < 4; ++e) {
+                const T x = tile[base | dpos(4 * p + e)];
+                split_tf32(x.x, hi[2 * e], lo[2 * e]);
+                split_tf32(x.y, hi[2 * e + 1], lo[2 * e + 1]);
             }
-        const uint32_t pin[4] = {dpos(tig), dpos(tig + 4), dpos(tig + 8), dpos(tig + 12)};
-        const uint32_t q0 = dpos(gid), q1 = dpos(gid + 8);
-        for (uint32_t nt = (uint32_t)tid >> 5; nt < NT; nt += (uint32_t)nthr >> 5) {
-            const uint32_t bi = gbase(nt * 8 + gid);
-            // B fragments: k-half kh holds inputs tig + 8 kh (b0) and tig + 4 + 8 kh (b1)
-            uint32_t rh[4], rl[4], dh[4], dl[4], sh[4], sl[4];  // xr, xi - xr, xr + xi
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const T x = tile[bi | pin[q]];
-                split_tf32(x.x, rh[q], rl[q]);
-                split_tf32(x.y - x.x, dh[q], dl[q]);
-                split_tf32(x.x + x.y, sh[q], sl[q]);
-            }
-            float k1[4] = {0.f, 0.f, 0.f, 0.f}, k2[4] = {0.f, 0.f, 0.f, 0.f}, k3[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int kh = 0; kh < 2; ++kh) {
-                const int b0 = 2 * kh, b1 = 2 * kh + 1;
-                mma_tf32(k1, al[0][kh], rh[b0], rh[b1]);
-                mma_tf32(k1, ah[0][kh], rl[b0], rl[b1]);
-                mma_tf32(k2, al[1][kh], dh[b0], dh[b1]);
-                mma_tf32(k2, ah[1][kh], dl[b0], dl[b1]);
-                mma_tf32(k3, al[2][kh], sh[b0], sh[b1]);
-                mma_tf32(k3, ah[2][kh], sl[b0], sl[b1]);
-                mma_tf32(k1, ah[0][kh], rh[b0], rh[b1]);
-                mma_tf32(k2, ah[1][kh], dh[b0], dh[b1]);
-                mma_tf32(k3, ah[2][kh], sh[b0], sh[b1]);
-            }
-            __syncwarp();
+            tmem_st8(cols + 8 * p, hi);
+            tmem_st8(cols + 32 + 8 * p, lo);
+        }
+        tmem_wait_st();
+        tc_fence_before();
+        csync();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t bsm = smem_u32(fuse + TC::dense_b_offset(K.stages));
 #pragma unroll
             for (uint32_t c = 0; c < 2; ++c) {
-                const uint32_t bo = gbase(nt * 8 + 2 * tig + c);
-                tile[bo | q0] = make_float2(k1[c] - k3[c], k1[c] + k2[c]);
-                tile[bo | q1] = make_float2(k1[2 + c] - k3[2 + c], k1[2 + c] + k2[2 + c]);
+                const uint32_t a = tmem + c * 96u, d = a + 64u;
+#pragma unroll
+                for (uint32_t st = 0; st < 4; ++st) umma_tf32(d, a + 8 * st, dense_b_desc(bsm + 1024 * st), st);
+#pragma unroll
+                for (uint32_t st = 0; st < 4; ++st) umma_tf32(d, a + 32 + 8 * st, dense_b_desc(bsm + 1024 * st), 1);
+#pragma unroll
+                for (uint32_t st = 0; st < 4; ++st)
+                    umma_tf32(d, a + 8 * st, dense_b_desc(bsm + 4096 + 1024 * st), 1);
             }
+            umma_commit(bar);
         }
+        uint32_t got = 0;
+        for (uint32_t it = 0; it < (1u << 20) && !got; ++it) got = mbar_try_wait(bar, state & 1u);
+        bool failed;
+        if constexpr (Grp::kWS)
+            failed = bar_or_first(blockDim.x - 32u, !got);
+        else
+            failed = __syncthreads_or(!got) != 0;
+        if (failed) {
+            if (tid == 0) {
+                slot[3] = state | (1u << 31);
+                if (atomicCAS(K.error_word, 0, DEV_ERR_TIMEOUT) == 0 && K.error_info) {
+                    K.error_info[0] = cur_site;
+                    K.error_info[1] = cur_pc;
+                    K.error_info[6] = 3000;  // the dense block's MMAs
+                }
+            }
+            stop = true;
+            return;
+        }
+        tc_fence_after();
+        uint32_t y[32];
+        tmem_ld32(cols + 64, y);
+        tmem_wait_ld();
+#pragma unroll
+        for (uint32_t d = 0; d < 16; ++d)
+            tile[base | dpos(d)] = make_float2(__uint_as_float(y[2 * d]), __uint_as_float(y[2 * d + 1]));
+        tc_fence_before();
+        if (tid == 0) slot[3] = state ^ 1u;  // read by the next call after the caller's barrier
     }
 
     // Whether instruction pc touches the statevector (needs every thread of a
@@ -3326,6 +3416,27 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
         }
         __syncthreads();
     }
+    // dense blocks: the MMA mbarrier and the CTA's TMEM columns, held for the
+    // whole launch (two CTAs per SM use all 512 columns)
+    constexpr bool kDenseKernel = sizeof(R) == 4 && G <= 0;
+    const bool dense = kDenseKernel && (K.flags & KF_DENSE) && fz != nullptr;
+    uint32_t* dslot = dense ? reinterpret_cast<uint32_t*>(fz + TileCfg<R, true>::kDenseSlotOffset) : nullptr;
+    if constexpr (kDenseKernel) {
+        if (dense) {
+            if (threadIdx.x == 0) {
+                mbar_init(reinterpret_cast<uint64_t*>(dslot), 1);
+                mbar_fence_init();
+                dslot[3] = 0;
+            }
+            if (threadIdx.x < 32) {
+                tmem_alloc(smem_u32(dslot + 2), kDenseTmemCols);
+                tmem_relinquish();
+            }
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+        }
+    }
     T* v;
     if (K.state_in_smem) {
         v = reinterpret_cast<T*>(rbase) + Grp::slot();
@@ -3357,6 +3468,16 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
             s.run(tally);
         }
         if (!Grp::kCta) __syncwarp();
+    }
+    if constexpr (kDenseKernel) {
+        if (dense) {
+            tc_fence_before();
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                tc_fence_after();
+                tmem_dealloc(dslot[2], kDenseTmemCols);
+            }
+        }
     }
     // flush per-lane totals (only group leaders hold non-zero values)
     if (tally.passed) atomicAdd(K.counters + 0, tally.passed);
