@@ -341,6 +341,7 @@ struct LaunchPlan {
     bool tiles;       // statevector passes stream through the bulk-copy tile engine
     bool fuse;        // ... and consecutive opcodes fuse into one pass
     uint32_t stages;  // tile buffers per CTA (2 / 3 let three 128-thread / two 256-thread CTAs share an SM)
+    bool dense;       // the kernel instance with tensor-core dense blocks (FP32, CTA groups, three stages)
 };
 
 uint32_t nw_template(uint32_t nw) { return nw <= 1 ? 1 : 4; }
@@ -456,6 +457,10 @@ PlanShape plan_shape(const clifft_gpu_program& p, uint32_t precision, uint32_t g
     L.tiles = (G == 0 || G == 32) && !L.state_in_smem;
     if (!L.tiles) L.stages = 0;
     L.fuse = L.tiles && allow_fusion;
+    // dense blocks: only in their own kernel instance (the others hold no
+    // tcgen05 instruction), for FP32 CTA groups of 256 compute threads
+    L.dense = dense && L.fuse && G == 0 && precision == CLIFFT_GPU_FP32 && L.stages == 3;
+    if (L.dense) L.fn = kernel_f32(ws_shape(uint32_t(L.threads)) ? -1 : 0, int(L.nw_words), true);
     L.smem = region_bytes(L.state_in_smem) * L.regions + tail(L.threads);
     if (L.smem > smem_cap) invalid("measurement record too large for shared memory");
     {
@@ -961,7 +966,7 @@ void sample_impl(clifft_gpu_program* prog, const clifft_gpu_sample_args* args, c
             // dense blocks on the tensor cores: FP32 CTA groups of 256 compute
             // threads (three tile stages) streaming fused blocks; other shapes
             // run the same blocks on the CUDA cores
-            const bool dense_ok = want_dense && Lx.G == 0 && Lx.fuse && Lx.stages == 3;
+            const bool dense_ok = Lx.dense;
             if (!dense_ok) Kx.flags &= ~uint32_t(KF_DENSE);
             Kx.fuse_bytes = Lx.tiles ? tile_scratch_bytes(args->precision, Lx.G == 0, Lx.stages, dense_ok) : 0;
             Kx.stages = Lx.stages;

@@ -653,7 +653,7 @@ struct CtlState {
 constexpr uint32_t kCtlBytes = 512;
 
 // --------------------------------------------------------------- the shot
-template <typename R, class Grp, int NW>
+template <typename R, class Grp, int NW, bool DENSE = false>
 struct Shot {
     using T = typename Cx<R>::T;
     static constexpr int S = Grp::S;
@@ -2168,6 +2168,20 @@ struct Shot {
     // 1) EXPANDs join the block and an active measurement ends it. Returns
     // the number of instructions consumed, 0 when the opcode at `pc` does not
     // start a block worth streaming.
+    // A fused block, in its dense-block instance when the launch asked for
+    // tensor-core dense blocks: the default instance carries none of that
+    // code, so its register allocation is the plain one. Kernels without
+    // DENSE contain no tcgen05 instruction at all: the instance that holds a
+    // TMEM allocation ran one CTA per SM at a time where shared memory and
+    // registers fit two (296 shots took twice as long as 148), and merely
+    // carrying that code slowed the default k = 24 path by 37 %.
+    __device__ __forceinline__ uint32_t run_block(uint32_t pc, int max_ops, uint32_t limit) {
+        if constexpr (kDenseOk) {
+            if (K.flags & KF_DENSE) return fused_block<true>(pc, max_ops, limit);
+        }
+        return fused_block<false>(pc, max_ops, limit);
+    }
+    template <bool WITH_DENSE>
     __device__ uint32_t fused_block(uint32_t pc, int max_ops, uint32_t limit) {
         constexpr uint32_t MB = TC::kBits;
         const bool wide = max_ops > 1;
@@ -2301,24 +2315,22 @@ struct Shot {
             red_bit = red_local ? (uint32_t)__popcll(F & ((1ull << tt) - 1)) : tt;
         }
         resolving = false;
-        if constexpr (kDenseOk) {
-            if (K.flags & KF_DENSE) {
-                Grp::sync();  // the resolved micro-ops, read by every thread
-                MOp* mm = reinterpret_cast<MOp*>(fuse + fuse_mops_offset());
-                uint32_t dmask = 0;
-                int j1 = 0;
-                const int j0 = find_dense(mm, n_body, (int)K.dense_min_weight, local_mask(fresh), dmask, j1);
-                if (j0 >= 0) {
-                    if (Grp::rank() < 16)
-                        compose_dense(mm, j0, j1, dmask, Grp::rank(),
-                                      reinterpret_cast<float*>(fuse + TC::dense_b_offset(K.stages)));
-                    fence_async_shared();  // the B operand, read by the tensor cores
-                    Grp::sync();
-                    if (Grp::rank() == 0) {
-                        mm[j0].kind = M_DENSE;
-                        mm[j0].req = dmask;
-                        for (int j = j0 + 1; j < j1; ++j) mm[j].kind = M_NOP;
-                    }
+        if constexpr (kDenseOk && WITH_DENSE) {
+            Grp::sync();  // the resolved micro-ops, read by every thread
+            MOp* mm = reinterpret_cast<MOp*>(fuse + fuse_mops_offset());
+            uint32_t dmask = 0;
+            int j1 = 0;
+            const int j0 = find_dense(mm, n_body, (int)K.dense_min_weight, local_mask(fresh), dmask, j1);
+            if (j0 >= 0) {
+                if (Grp::rank() < 16)
+                    compose_dense(mm, j0, j1, dmask, Grp::rank(),
+                                  reinterpret_cast<float*>(fuse + TC::dense_b_offset(K.stages)));
+                fence_async_shared();  // the B operand, read by the tensor cores
+                Grp::sync();
+                if (Grp::rank() == 0) {
+                    mm[j0].kind = M_DENSE;
+                    mm[j0].req = dmask;
+                    for (int j = j0 + 1; j < j1; ++j) mm[j].kind = M_NOP;
                 }
             }
         }
@@ -2339,7 +2351,7 @@ struct Shot {
         const int nmo = term_kind >= 2 ? nm - 1 : nm;
         auto body = [&](T* buf, uint64_t, uint64_t tbase) {
             for (int j = 0; j < nmo;) {
-                if constexpr (kDenseOk) {
+                if constexpr (kDenseOk && WITH_DENSE) {
                     if (mops[j].kind == M_NOP) {
                         ++j;
                         continue;
@@ -2709,7 +2721,8 @@ struct Shot {
     }
 
     // ---- dense blocks on the tensor cores (KF_DENSE, FP32 CTA groups)
-    static constexpr bool kDenseOk = sizeof(R) == 4 && Grp::kCta;
+    // the dense-block code exists only in the kernel instances built for it
+    static constexpr bool kDenseOk = DENSE && sizeof(R) == 4 && Grp::kCta;
     // Tile-local bits a micro-op moves or reads, or ~0u when it cannot join a
     // dense run (an expansion, a renormalisation, a condition on tile-global
     // bits).
@@ -2895,7 +2908,7 @@ struct Shot {
     // D and writes its group back. The waits of all compute threads agree;
     // a wait that gives up records a device error and turns the dense path
     // off for the rest of the launch on this CTA.
-    __device__ void apply_dense(uint32_t dmask, T* tile, int tid) {
+    __device__ __noinline__ void apply_dense(uint32_t dmask, T* tile, int tid) {
         uint32_t* slot = reinterpret_cast<uint32_t*>(fuse + TC::kDenseSlotOffset);
         uint64_t* bar = reinterpret_cast<uint64_t*>(slot);
         const uint32_t state = slot[3];  // bit 0: the mbarrier's phase, bit 31: off after a timeout
@@ -3069,7 +3082,7 @@ struct Shot {
     // a statevector step executed by every thread (fused block or one opcode)
     __device__ __forceinline__ uint32_t run_all(uint32_t pc, bool fuse_on) {
         uint32_t used = 0;
-        if (tiled(k)) used = fused_block(pc, fuse_on ? TC::kMops : 1, P.n_instr);
+        if (tiled(k)) used = run_block(pc, fuse_on ? TC::kMops : 1, P.n_instr);
         if (!used) {
             exec(pc);
             used = 1;
@@ -3146,7 +3159,7 @@ struct Shot {
                 if constexpr (kTiles) {
                     // a warp running one shot streams its global statevector
                     // through the tile engine like a CTA group
-                    if (tiled(k)) used = fused_block(pc, max_ops, end);
+                    if (tiled(k)) used = run_block(pc, max_ops, end);
                 }
                 if (!used) {
                     exec(pc);
@@ -3383,7 +3396,7 @@ __host__ __device__ constexpr int shots_per_group_region() {
     return G <= 0 ? 1 : 32 / G;
 }
 
-template <typename R, int G, int NW>
+template <typename R, int G, int NW, bool DENSE = false>
 __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1 : 4)
     svm_sample_kernel(const DevProg P, const KParams K) {
     using Grp = typename GroupOf<G>::type;
@@ -3410,7 +3423,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
         // warp): initialised once, reused by every pass of every shot the
         // group runs
         if (Grp::rank() == 0) {
-            uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW>::fuse_bar_offset());
+            uint64_t* bars = reinterpret_cast<uint64_t*>(fz + Shot<R, Grp, NW, DENSE>::fuse_bar_offset());
             for (int st = 0; st < 2 * kMaxStages; ++st) mbar_init(&bars[st], 1);
             mbar_fence_init();
         }
@@ -3418,7 +3431,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
     }
     // dense blocks: the MMA mbarrier and the CTA's TMEM columns, held for the
     // whole launch (two CTAs per SM use all 512 columns)
-    constexpr bool kDenseKernel = sizeof(R) == 4 && G <= 0;
+    constexpr bool kDenseKernel = DENSE && sizeof(R) == 4 && G <= 0;
     const bool dense = kDenseKernel && (K.flags & KF_DENSE) && fz != nullptr;
     uint32_t* dslot = dense ? reinterpret_cast<uint32_t*>(fz + TileCfg<R, true>::kDenseSlotOffset) : nullptr;
     if constexpr (kDenseKernel) {
@@ -3464,7 +3477,7 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
         const unsigned long long item = base + Grp::slot();
         if (item < n_items) {
             const unsigned long long shot = K.seg_in ? (unsigned long long)K.seg_in[item] : item;
-            Shot<R, Grp, NW> s(P, K, v, rec, det, obs, red, fz, &bar_phase, shot);
+            Shot<R, Grp, NW, DENSE> s(P, K, v, rec, det, obs, red, fz, &bar_phase, shot);
             s.run(tally);
         }
         if (!Grp::kCta) __syncwarp();

@@ -3,5 +3,12 @@
 #include "svm_instantiate.cuh"
 
 namespace cgpu {
-KernelFn kernel_f32(int G, int nw) { return pick_kernel_impl<float>(G, nw); }
+// FP32 one-CTA-per-shot kernels with the tensor-core dense blocks
+static KernelFn pick_dense_f32(int G, int nw) {
+    if (G < 0) return nw <= 1 ? svm_sample_kernel<float, -1, 1, true> : svm_sample_kernel<float, -1, 4, true>;
+    return nw <= 1 ? svm_sample_kernel<float, 0, 1, true> : svm_sample_kernel<float, 0, 4, true>;
+}
+KernelFn kernel_f32(int G, int nw, bool dense) {
+    return dense && G <= 0 ? pick_dense_f32(G, nw) : pick_kernel_impl<float>(G, nw);
+}
 }  // namespace cgpu
