@@ -566,11 +566,12 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
 // groups for L2/HBM-resident ones up to 4 MiB, and for larger statevectors
 // CTAs of 128 (two tile buffers, three CTAs per SM), 256 (three buffers, two
 // per SM), 512 threads (four buffers) or 256 / 512 + a copy warp (three /
-// four buffers, warp-specialised fused blocks). Up to 8 MiB a warp per shot
+// four buffers, warp-specialised fused blocks). Up to 16 MiB a warp per shot
 // is tried too: with thousands of shots resident (16 warps per SM) it beats
-// every CTA shape (k = 20, 2368 shots: 715 vs 986 ms), with fewer it loses
-// (1184 shots: 563 vs 486 ms); at k = 24 it loses at any count (2368 shots:
-// 789 vs 3074 shots/s). The trial runs on the call's own shots decide.
+// every CTA shape (2368 shots: k = 20 715 vs 986 ms, k = 21 1353 vs 1797 ms),
+// with fewer it loses (k = 20, 1184 shots: 563 vs 486 ms); from k = 22 on it
+// loses at any count (k = 22: 4486 vs 3663 ms; k = 24: 789 vs 3074 shots/s).
+// The trial runs on the call's own shots decide.
 std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t precision) {
     const size_t amp = precision == CLIFFT_GPU_FP32 ? 8 : 16;
     const size_t state_bytes = (size_t(1) << p.meta.peak_rank) * amp;
@@ -581,7 +582,7 @@ std::vector<uint32_t> tune_candidates(const clifft_gpu_program& p, uint32_t prec
             if (x >= 1 && x <= 32) c.push_back(uint32_t(x));
     } else if (state_bytes <= (size_t(4) << 20)) {
         c = {32, 16, 64, 128, 256};
-    } else if (state_bytes <= (size_t(8) << 20)) {
+    } else if (state_bytes <= (size_t(16) << 20)) {
         c = {32, 128, 256, 512, kWsThreadsHalf, kWsThreads};
     } else {
         c = {128, 256, 512, kWsThreadsHalf, kWsThreads};
