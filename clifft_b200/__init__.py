@@ -15,11 +15,11 @@ include/clifft_gpu.h:
 from .program import OP, OPCODES, Program
 from ._sample_result import SampleResult
 from .api import (DeviceProgram, compute_reference_syndrome, load, noise_site_probabilities,
-                  record_probabilities, run, sample, sample_k, sample_k_survivors, sample_survivors)
+                  record_probabilities, run, sample, sample_k, sample_k_survivors, sample_survivors, trim)
 from ._native import backend_name
 
 __all__ = [
     "OP", "OPCODES", "Program", "SampleResult", "DeviceProgram", "load", "run", "sample",
     "sample_survivors", "sample_k", "sample_k_survivors", "noise_site_probabilities",
-    "record_probabilities", "compute_reference_syndrome", "backend_name",
+    "record_probabilities", "compute_reference_syndrome", "trim", "backend_name",
 ]

@@ -88,6 +88,8 @@ def lib():
             L.clifft_gpu_load.argtypes = [P, ctypes.POINTER(P)]
             L.clifft_gpu_free.restype = None
             L.clifft_gpu_free.argtypes = [P]
+            L.clifft_gpu_trim.restype = None
+            L.clifft_gpu_trim.argtypes = []
             L.clifft_gpu_sample.restype = ctypes.c_int
             L.clifft_gpu_sample.argtypes = [P, ctypes.POINTER(SampleArgs), ctypes.POINTER(Outputs)]
             L.clifft_gpu_sample_noalloc.restype = ctypes.c_int
@@ -120,7 +122,7 @@ EXPORTED_SYMBOLS = (
     "clifft_gpu_load", "clifft_gpu_free", "clifft_gpu_sample", "clifft_gpu_backend_name",
     "clifft_gpu_last_error", "clifft_gpu_program_peak_rank", "clifft_gpu_program_device_bytes",
     "clifft_gpu_sample_noalloc", "clifft_gpu_batch_create", "clifft_gpu_batch_run", "clifft_gpu_batch_free",
-    "clifft_gpu_expval_grad", "clifft_gpu_program_num_rot_params", "clifft_gpu_sample_k",
+    "clifft_gpu_expval_grad", "clifft_gpu_program_num_rot_params", "clifft_gpu_sample_k", "clifft_gpu_trim",
 )
 NOALLOC_SCRATCH_WORDS = 512  # CLIFFT_GPU_NOALLOC_SCRATCH_WORDS
 

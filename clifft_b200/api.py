@@ -246,6 +246,12 @@ def _survivor_result(p: Program, r: Dict[str, object], keep_records: bool, shots
                         exp_vals=ev, stats=_stats(r))
 
 
+def trim() -> None:
+    """Return the statevector slabs that released programs left parked for
+    the next upload (clifft_gpu_trim) to the device."""
+    N.lib().clifft_gpu_trim()
+
+
 def compute_reference_syndrome(program: Program, *, precision: str = "fp64") -> Dict[str, np.ndarray]:
     """Noiseless reference syndrome: the detector and observable parities of
     one noise-free shot with seed 0 (clifft::compute_reference_syndrome,
