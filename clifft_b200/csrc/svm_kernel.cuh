@@ -3487,6 +3487,13 @@ __global__ void __launch_bounds__(G == 0 ? 512 : (G < 0 ? 544 : 128), G <= 0 ? 1
             tc_fence_before();
             __syncthreads();
             if (threadIdx.x < 32) {
+                // after a timed-out wait: wait (bounded) for the MMAs still in
+                // flight before their TMEM columns are released
+                const uint32_t st = dslot[3];
+                if (st >> 31)
+                    for (uint32_t it = 0; it < (1u << 20); ++it)
+                        if (mbar_try_wait(reinterpret_cast<uint64_t*>(dslot), st & 1u)) break;
+                __syncwarp();  // the dealloc is warp-aligned
                 tc_fence_after();
                 tmem_dealloc(dslot[2], kDenseTmemCols);
             }
