@@ -227,6 +227,21 @@ uint32_t validate(const clifft_program_image& im) {
 }
 
 
+// Returns the current device's parked spare slab to the device (defined with
+// the spare slabs below); true when there was one.
+bool spare_release_current();
+// A device allocation that, when the device is out of memory, returns the
+// parked spare slab and tries once more.
+template <class Alloc>
+cudaError_t alloc_retry(Alloc&& alloc) {
+    cudaError_t e = alloc();
+    if (e == cudaErrorMemoryAllocation && spare_release_current()) {
+        cudaGetLastError();  // clear the failed allocation's error
+        e = alloc();
+    }
+    return e;
+}
+
 // Device-side scratch freed in stream order when the call ends.
 struct StreamBuffers {
     cudaStream_t stream;
@@ -235,7 +250,7 @@ struct StreamBuffers {
     void* alloc(size_t bytes) {
         void* p = nullptr;
         if (bytes == 0) return nullptr;
-        CUDA_OK(cudaMallocAsync(&p, bytes, stream));
+        CUDA_OK(alloc_retry([&] { return cudaMallocAsync(&p, bytes, stream); }));
         ptrs.push_back(p);
         return p;
     }
@@ -320,6 +335,20 @@ void spare_park(int device, void* ptr, size_t bytes) {
     }
     if (drop) cudaFree(drop);
 }
+bool spare_release_current() {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return false;
+    void* ptr = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_spare_mu);
+        auto it = g_spare.find(device);
+        if (it == g_spare.end()) return false;
+        ptr = it->second.first;
+        g_spare.erase(it);
+    }
+    cudaFree(ptr);
+    return true;
+}
 size_t spare_bytes(int device) {
     std::lock_guard<std::mutex> lock(g_spare_mu);
     auto it = g_spare.find(device);
@@ -348,7 +377,7 @@ struct SlabLease {
                 prog.slab = sp;
                 prog.slab_bytes = got;
             } else {
-                CUDA_OK(cudaMalloc(&prog.slab, bytes));
+                CUDA_OK(alloc_retry([&] { return cudaMalloc(&prog.slab, bytes); }));
                 prog.slab_bytes = bytes;
             }
         }
@@ -839,7 +868,7 @@ int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out)
             const uint8_t op = p->instr_host[size_t(i) * 32];
             if (op == CLIFFT_OP_ARRAY_ROT || op == CLIFFT_OP_EXPAND_ROT) ++p->num_rot_params;
         }
-        CUDA_OK(cudaMalloc(&p->blob, b.bytes.size()));
+        CUDA_OK(alloc_retry([&] { return cudaMalloc(&p->blob, b.bytes.size()); }));
         p->blob_bytes = b.bytes.size();
         CUDA_OK(cudaMemcpy(p->blob, b.bytes.data(), b.bytes.size(), cudaMemcpyHostToDevice));
         DevProg& d = p->dev;
@@ -1553,12 +1582,12 @@ int clifft_gpu_batch_create(clifft_gpu_program* const* progs, const clifft_gpu_s
                 const size_t amp = a.precision == CLIFFT_GPU_FP32 ? 8 : 16;
                 const size_t bytes = size_t(it.L.blocks) * it.L.regions * it.L.S * it.L.state_stride * amp;
                 slab_total += bytes;
-                CUDA_OK(cudaMalloc(&it.slab, bytes));
+                CUDA_OK(alloc_retry([&] { return cudaMalloc(&it.slab, bytes); }));
                 K.state_global = it.slab;
             }
         }
         (void)slab_total;
-        CUDA_OK(cudaMalloc(&b->scratch_block, words * 8));
+        CUDA_OK(alloc_retry([&] { return cudaMalloc(&b->scratch_block, words * 8); }));
         b->scratch_block_words = words;
         CUDA_OK(cudaGraphCreate(&b->graph, 0));
         for (auto& it : b->items) {
