@@ -299,7 +299,9 @@ namespace {
 std::mutex g_spare_mu;
 std::map<int, std::pair<void*, size_t>> g_spare;  // device -> (slab, bytes)
 
-// takes the device's spare when it holds at least `bytes` (else frees it)
+// takes the device's spare when it holds `bytes` without wasting more than
+// as much again; a smaller spare is freed, a much larger one stays parked
+// (an allocation that runs out of memory releases it)
 void* spare_take(int device, size_t bytes, size_t* got) {
     void* ptr = nullptr;
     size_t have = 0;
@@ -307,8 +309,9 @@ void* spare_take(int device, size_t bytes, size_t* got) {
         std::lock_guard<std::mutex> lock(g_spare_mu);
         auto it = g_spare.find(device);
         if (it == g_spare.end()) return nullptr;
-        ptr = it->second.first;
         have = it->second.second;
+        if (have > 2 * bytes) return nullptr;
+        ptr = it->second.first;
         g_spare.erase(it);
     }
     if (have >= bytes) {
@@ -348,11 +351,6 @@ bool spare_release_current() {
     }
     cudaFree(ptr);
     return true;
-}
-size_t spare_bytes(int device) {
-    std::lock_guard<std::mutex> lock(g_spare_mu);
-    auto it = g_spare.find(device);
-    return it == g_spare.end() ? 0 : it->second.second;
 }
 
 struct SlabLease {
@@ -636,7 +634,6 @@ LaunchPlan plan_launch(const clifft_gpu_program& p, uint32_t precision, uint32_t
         // global slabs: bound the resident state to ~half of free HBM
         size_t free_b = 0, total_b = 0;
         CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
-        free_b += spare_bytes(p.device);  // a parked slab is this library's to reuse
         uint64_t per_block_bytes = uint64_t(state_bytes) * shots_per_block;
         uint64_t max_blocks = std::max<uint64_t>(1, (free_b / 2) / std::max<uint64_t>(per_block_bytes, 1));
         blocks = std::min<uint64_t>(blocks, max_blocks);
