@@ -291,11 +291,10 @@ namespace {
 // A call's use of the program's statevector slab: the first request takes the
 // cached slab (growing it if needed); later requests of the same call reuse
 // it, since the call's launches run one after another on one stream.
-// One spare statevector slab per device: a released program parks its slab
-// here and the next program's first sampling call takes it over, so
-// re-uploading a program does not pay the mapping of tens of GB again
-// (k = 24, 296 shots: 38 GB, 4-7 ms to allocate, ~20 ms to free).
-// clifft_gpu_trim returns it to the device.
+// One spare statevector slab per device, taken over by a program's first
+// sampling call when it fits. Released programs free their slabs (parking
+// them here made the 64-program batch graph 20x slower, cause not found), so
+// the pool stays empty unless a caller fills it; clifft_gpu_trim empties it.
 std::mutex g_spare_mu;
 std::map<int, std::pair<void*, size_t>> g_spare;  // device -> (slab, bytes)
 
@@ -320,23 +319,6 @@ void* spare_take(int device, size_t bytes, size_t* got) {
     }
     cudaFree(ptr);
     return nullptr;
-}
-// parks a slab no launch uses any more (keeps the larger of two)
-void spare_park(int device, void* ptr, size_t bytes) {
-    void* drop = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_spare_mu);
-        auto it = g_spare.find(device);
-        if (it == g_spare.end()) {
-            g_spare[device] = {ptr, bytes};
-        } else if (it->second.second < bytes) {
-            drop = it->second.first;
-            it->second = {ptr, bytes};
-        } else {
-            drop = ptr;
-        }
-    }
-    if (drop) cudaFree(drop);
 }
 bool spare_release_current() {
     int device = 0;
@@ -921,7 +903,7 @@ void clifft_gpu_free(clifft_gpu_program* prog) {
     if (prog->blob || prog->slab) {
         cudaDeviceSynchronize();
         if (prog->blob) cudaFree(prog->blob);
-        if (prog->slab) spare_park(prog->device, prog->slab, prog->slab_bytes);
+        if (prog->slab) cudaFree(prog->slab);
     }
     delete prog;
 }

@@ -144,12 +144,10 @@ typedef struct clifft_gpu_outputs {
 
 /* Upload + validate a program. *out receives an opaque handle. */
 int clifft_gpu_load(const clifft_program_image* image, clifft_gpu_program** out);
-/* Release a handle (waits for the device). The statevector slab that
- * sampling calls keep on it between calls is parked as the device's spare:
- * the next program's first sampling call takes it over instead of mapping
- * tens of GB again (one spare per device, the larger one kept). */
+/* Release a handle (waits for the device) and the statevector slab that
+ * sampling calls keep on it between calls. */
 void clifft_gpu_free(clifft_gpu_program* prog);
-/* Return the parked spare slabs of every device to the device. */
+/* Return any spare statevector slab the library holds to the device. */
 void clifft_gpu_trim(void);
 /* Sample. See the flags above for survivors / forced / trace behaviour.
  * Survivor compaction: with CLIFFT_GPU_SURVIVORS, at least four resident waves
