@@ -1,7 +1,7 @@
-"""Reuse of a released program's statevector slab (clifft_gpu_free parks it
-as the device's spare; the next program's first sampling call takes it over;
-clifft_gpu_trim returns it). Each shot initialises its own state, so records
-must not depend on what the slab held before."""
+"""Statevector slabs across program uploads: a program uploaded again after
+others ran (and were released) samples the same records, and clifft_gpu_trim
+is safe to call at any point. Each shot initialises its own state, so records
+must not depend on what device memory held before."""
 
 from __future__ import annotations
 
@@ -24,9 +24,9 @@ def test_parked_slab_serves_the_next_upload(name, group):
     shots = 300
     first = Program.load(path)
     want = cb.run(first, shots, 21, precision="fp32", group_threads=group)
-    first._device_program.free()  # parks the slab
+    first._device_program.free()
     other = Program.load(os.path.join(PROGRAMS, "cfg2_01.npz"))
-    cb.run(other, 64, 3, precision="fp32")  # takes (or replaces) the spare, dirties it
+    cb.run(other, 64, 3, precision="fp32")  # other statevectors in device memory
     other._device_program.free()
     again = Program.load(path)
     got = cb.run(again, shots, 21, precision="fp32", group_threads=group)
